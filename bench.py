@@ -1,0 +1,438 @@
+#!/usr/bin/env python3
+"""Benchmark of the DynaMOSP update path on one B200 (or N replicas).
+
+Workload (the road-network configuration): a 1404 x 1404 grid whose edges
+are kept with p = 0.70, 1% of the vertices with one diagonal shortcut, the
+largest connected component (~1.9M vertices, ~5.4M directed edges); K = 3
+objectives with weights U[1,100] (seed 12345); source 0; Pref = (1,1,1);
+50,000 changes, 50% insertions, connectivity-safe deletions (seed 777, the
+reference generator's uniform mode). Synthetic stand-in for SuiteSparse
+roadNet-CA, which is not available here.
+
+One step = one MOSP update: the K SOSP updates (one fused persistent launch)
+plus Steps 2-3 (combined graph + its SSSP, a second launch) - the region the
+reference reports as gpu_compute_ms. Metric: changed edges (applied inserts
++ deletes) per second of that region. `value` has inputs resident in HBM
+(each step restores the initial trees on the device and flushes L2 before its
+timed region); `e2e` runs the same update through mosp_update_host with host
+buffers (batch application, upload, GPU work, path costs and download inside
+the timed region).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun every rank runs the same workload on its own GPU (replicas:
+one update does not shard); value = all ranks' changed edges / the slowest
+rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "mosp-cuda_b200"))
+
+METRIC = "MOSP update changed-edges/s (K SOSP updates + combined graph + its SSSP)"
+UNIT = "changed-edges/s"
+WORKLOAD = ("road-network shape: 1404x1404 grid, edges kept p=0.70, 1% diagonal shortcuts, largest "
+            "component; K=3 weights U[1,100] seed 12345; source 0; Pref=(1,1,1); 50,000 changes, 50% "
+            "insertions, connectivity-safe deletions, seed 777")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--width", type=int, default=1404)
+    ap.add_argument("--changes", type=int, default=50000)
+    ap.add_argument("--delta", type=int, default=0, help="fixed near-far width (0: default heuristic)")
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--verify", action="store_true", help="check the result against the oracle")
+    return ap.parse_args()
+
+
+def make_workload(args):
+    import mosp_b200 as mb
+    g = mb.HostGraph.grid_road(args.width, args.width, 0.70, 0.01, 3, 1, 100, 12345)
+    batch = mb.HostBatch.generate(g, args.changes, 50.0, "uniform", 0, True, 777, 0, 1, 100)
+    return g, batch
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock and throttle-reason samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.proc = None
+        self.path = None
+        self.device_index = device_index
+        if shutil.which("nvidia-smi") is None:
+            return
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                      "-i", str(device_index), "-lms", "200"], stdout=open(self.path, "w"),
+                                     stderr=subprocess.DEVNULL)
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import datetime
+
+    import torch
+    import mosp_b200 as mb
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    g, batch = make_workload(args)
+    K, n, src = 3, g.n, 0
+    ws = mb.Workspace(timeout_ms=60000)
+    ws.enable_timing(True)
+    row, col, w = g.arrays()
+    # initial canonical trees of the original graph (GPU engine, from scratch)
+    dg0 = mb.DeviceGraph.upload(ws, g)
+    d0 = torch.empty((K, n), dtype=torch.int64, device="cuda")
+    p0 = torch.empty((K, n), dtype=torch.int32, device="cuda")
+    maxw_orig = [int(w[:, k].max()) for k in range(K)]
+    for k in range(K):
+        ws.sosp_from_scratch(n, g.m, dg0.out_row, dg0.out_col, dg0.out_w_col(k), src,
+                             mb.default_delta(g.m, n, int(w[:, k].sum())), maxw_orig[k], d0[k], p0[k])
+    del dg0
+    upd = mb.apply_batch(g, batch)
+    ba = batch.arrays()
+    changed = int(batch.n_ins + batch.n_del)
+    dg = mb.DeviceGraph.upload(ws, upd)
+    ch = mb.changed_lists(ba, K)
+    cf = torch.from_numpy(np.concatenate([c[0] for c in ch])).cuda()
+    ct = torch.from_numpy(np.concatenate([c[1] for c in ch])).cuda()
+    off = np.concatenate([[0], np.cumsum([len(c[0]) for c in ch])])
+    heads = torch.from_numpy(ba["ins_to"]).cuda()
+    maxw = [max(maxw_orig[k], int(ba["ins_w"][:, k].max())) for k in range(K)]
+    deltas = [args.delta if args.delta > 0 else mb.default_delta(g.m, n, int(w[:, k].sum())) for k in range(K)]
+    dist_t = torch.empty_like(d0)
+    par_t = torch.empty_like(p0)
+    cd = torch.empty(n, dtype=torch.int64, device="cuda")
+    cp = torch.empty(n, dtype=torch.int32, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def step(timed):
+        dist_t.copy_(d0)
+        par_t.copy_(p0)
+        flush.zero_()
+        if timed:
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+        stats, cst = ws.update_device(n, upd.m, K, dg.out_row, dg.out_col, dg.out_w, dg.in_row, dg.in_col, dg.in_w,
+                                      cf, ct, off, heads, len(ba["ins_to"]), src, deltas, maxw, None, dist_t, par_t,
+                                      cd, cp, stream=None)
+        if timed:
+            e.record(stream)
+            e.synchronize()
+            return s.elapsed_time(e), ws.last_timing(), stats, cst
+        return None
+
+    for _ in range(max(args.warmup, 0)):
+        step(False)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    clocks = ClockSampler(local)
+    torch.cuda.synchronize()
+    step_ms, upd_ms, comb_ms = [], [], []
+    stats = cst = None
+    wall0 = time.perf_counter()
+    for _ in range(args.steps):
+        ms, (um, cm), stats, cst = step(True)
+        step_ms.append(ms)
+        upd_ms.append(um)
+        comb_ms.append(cm)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - wall0
+    clock = clocks.stop()
+    total_ms = float(sum(step_ms))
+    if pg:
+        t = torch.tensor([total_ms], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_ms = float(t.item())
+        pg.barrier()
+    ms_per_step = total_ms / args.steps
+    value = world * changed * args.steps / (total_ms / 1000.0)
+
+    # roofline of the dominant kernel (the fused K-objective update)
+    old_d, old_p = d0.cpu().numpy(), p0.cpu().numpy()
+    new_d, new_p = dist_t.cpu().numpy(), par_t.cpu().numpy()
+    ab = mb.algorithmic_bytes(upd, batch, K, src, old_d, old_p, new_d, new_p, cst.edges)
+    peak, peak_kind = measured_peak()
+    upd_mean = float(np.mean(upd_ms))
+    comb_mean = float(np.mean(comb_ms))
+    achieved = ab["update"] / (upd_mean / 1000.0) / 1e9
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tfile):
+        try:
+            traffic = json.load(open(tfile)).get("sosp_update_bytes_per_launch")
+        except ValueError:
+            traffic = None
+    roofline = {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 5), "traffic": traffic,
+                "kernel": "sospEngine<update> (K=3 fused SOSP updates)",
+                "algorithmic_bytes_per_launch": ab["update"], "kernel_ms": round(upd_mean, 4),
+                "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
+                else "fallback 6650 GB/s",
+                "combined": {"kernel_ms": round(comb_mean, 4), "algorithmic_bytes_per_launch": ab["combined"],
+                             "achieved_gbs": round(ab["combined"] / (comb_mean / 1000.0) / 1e9, 2)}}
+
+    if args.verify:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as orc
+        exp = orc.expected_update((row, col, w), ba, K, src)
+        assert np.array_equal(new_d, exp["dist"]) and np.array_equal(new_p, exp["parent"])
+        assert np.array_equal(cd.cpu().numpy(), exp["comb_dist"]) and np.array_equal(cp.cpu().numpy(),
+                                                                                      exp["comb_parent"])
+
+    # end to end: host buffers through mosp_update_host
+    e2e = None
+    if args.e2e_steps > 0:
+        host_ws = mb.Workspace(timeout_ms=60000)
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+        garr = tuple(pin(x) for x in (row, col, w))
+        barr = {k: pin(v) for k, v in ba.items() if k != "mask"}
+        hd0, hp0 = pin(old_d), pin(old_p)
+        host_ws.update_host(garr, barr, hd0, hp0, K, src, costs=True)  # warm-up
+        times = []
+        for _ in range(args.e2e_steps):
+            t0 = time.perf_counter()
+            _, _, _, _, _, tm = host_ws.update_host(garr, barr, hd0, hp0, K, src, costs=True)
+            times.append(time.perf_counter() - t0)
+        e2e_s = float(np.mean(times))
+        if pg:
+            t = torch.tensor([e2e_s], device="cuda")
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        m_upd = upd.m
+        h2d = (n + 1 + m_upd) * 4 + m_upd * 3 * 4 + K * n * 12 + batch.n_ins * 4 + 2 * 4 * sum(len(c[0]) for c in ch)
+        d2h = K * n * 12 + n * 12 + n * 3 * 8
+        e2e = {"value": round(world * changed / e2e_s, 1), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e_s * 1000, 3),
+               "path": "mosp_update_host (host apply, upload, GPU update + combined + costs, download)",
+               "stages_ms": {k: round(getattr(tm, k), 3) for k in
+                             ("apply_batch", "upload", "objectives", "combined", "costs", "download")}}
+        host_ws.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_port(row, col, w, upd, ba, ch, old_d, old_p, K, src, changed)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "n": n, "m": upd.m, "K": K, "changes_applied": changed,
+                           "inserts": batch.n_ins, "deletes": batch.n_del, "parallelism": f"replicas x{world}",
+                           "delta": deltas, "l2": "flushed (256 MiB write) before every timed step",
+                           "grid_ctas": ws.grid()},
+                "gpu_compute_ms": round(ms_per_step, 4),
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 2 * args.steps,
+                "clocks": clock, "wall_s_timed_loop": round(wall, 4),
+                "stats": {"invalidated": [s.invalidated for s in stats], "iterations": [s.iterations for s in stats],
+                          "epochs": [s.epochs for s in stats], "pushes": [s.pushes for s in stats],
+                          "jump_rounds": stats[0].jump_rounds, "combined_edges": cst.edges,
+                          "combined_iterations": cst.search.iterations, "expanded": ab["expanded"]}}
+        print(json.dumps(line), flush=True)
+    ws.close()
+    if pg:
+        pg.destroy_process_group()
+
+
+def cpu_baseline_port(row, col, w, upd, ba, ch, old_d, old_p, K, src, changed):
+    """The oracle's restatement of the reference CPU path (sequential update
+    per objective, then the host combined graph + Dijkstra), one full
+    update, one thread."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    urow, ucol, uw = upd.arrays()
+    rrow, rcol, rw = orc.transpose(urow, ucol, uw)
+    t0 = time.perf_counter()
+    parents = []
+    for k in range(K):
+        d = old_d[k].copy()
+        p = old_p[k].copy()
+        n = len(urow) - 1
+        lib = orc.olib()
+        cf, ct = np.ascontiguousarray(ch[k][0]), np.ascontiguousarray(ch[k][1])
+        heads = np.ascontiguousarray(ba["ins_to"], np.int32)
+        lib.oracle_sequential_update(n, uw.shape[1], k, src, orc.P(urow), orc.P(ucol), orc.P(uw), orc.P(rrow),
+                                     orc.P(rcol), orc.P(rw), len(cf), orc.P(cf), orc.P(ct), len(heads),
+                                     orc.P(heads), orc.P(d), orc.P(p))
+        parents.append(p)
+    crow, ccol, cw = orc.combined_graph(np.stack(parents), len(urow) - 1, K, src, None)
+    orc.dijkstra(crow, ccol, cw, 0, src)
+    secs = time.perf_counter() - t0
+    return {"value": round(changed / secs, 1), "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": "one full MOSP update of the workload (K=3 sequential SOSP updates + host combined graph "
+                      f"+ Dijkstra), compute only, {secs:.2f} s"}
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the reference's own CPU implementation of the path
+# ---------------------------------------------------------------------------
+def run_reference(args):
+    world, rank, _ = dist_setup(args)
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    import mosp_b200 as mb
+    from concurrent.futures import ThreadPoolExecutor
+
+    g, batch = make_workload(args)
+    K, src = 3, 0
+    row, col, w = g.arrays()
+    ba = batch.arrays()
+    changed = int(batch.n_ins + batch.n_del)
+    have_ref = orc.have_ref()
+    tmp = tempfile.mkdtemp(prefix="mosp_ref_")
+    try:
+        prefix = os.path.join(tmp, "graph", "graphCsr")
+        g.write(prefix)
+        ins, dele = os.path.join(tmp, "insert.txt"), os.path.join(tmp, "delete.txt")
+        batch.write(ins, dele)
+        dijk = orc.ref_dijkstra if have_ref else orc.dijkstra
+        for k in range(K):
+            d, p = dijk(row, col, w, k, src)
+            mb.check(mb.lib().mosp_write_tree(os.path.join(tmp, f"d{k}.txt").encode(),
+                                              os.path.join(tmp, f"t{k}.txt").encode(), g.n, d.ctypes.data,
+                                              p.ctypes.data))
+        upd = mb.apply_batch(g, batch)
+        urow, ucol, uw = upd.arrays()
+        ch = mb.changed_lists(batch.arrays(), K)
+
+        def objective(k):
+            if have_ref:
+                ok = orc.ref_sequential_update(prefix, os.path.join(tmp, f"d{k}.txt"), os.path.join(tmp, f"t{k}.txt"),
+                                               ins, dele, k, src, os.path.join(tmp, f"od{k}.txt"),
+                                               os.path.join(tmp, f"ot{k}.txt"))
+                assert ok
+                p = np.empty(g.n, np.int32)
+                d = np.empty(g.n, np.int64)
+                mb.check(mb.lib().mosp_read_tree(os.path.join(tmp, f"od{k}.txt").encode(),
+                                                 os.path.join(tmp, f"ot{k}.txt").encode(), g.n, d.ctypes.data,
+                                                 p.ctypes.data))
+                return p
+            d0, p0 = orc.dijkstra(row, col, w, k, src)
+            return orc.sequential_update(urow, ucol, uw, k, src, ch[k][0], ch[k][1], ba["ins_to"], d0, p0)[1]
+
+        def one_step():
+            t0 = time.perf_counter()
+            with ThreadPoolExecutor(max_workers=K) as pool:
+                parents = list(pool.map(objective, range(K)))
+            if have_ref:
+                orc.ref_combined_dijkstra(np.stack(parents), g.n, K, src, None)
+            else:
+                crow, ccol, cw = orc.combined_graph(np.stack(parents), g.n, K, src, None)
+                orc.dijkstra(crow, ccol, cw, 0, src)
+            return time.perf_counter() - t0
+
+        first = one_step()  # warm-up (file cache, page faults)
+        budget = 200.0
+        steps = max(1, min(args.steps, int(budget / max(first, 1e-3))))
+        times = [one_step() for _ in range(steps)]
+        secs = float(np.mean(times))
+        value = changed / secs
+        kind = "reference" if have_ref else "port"
+        sample = (("reference sequentialSOSPUpdate (file API, text read/write included, as the reference's CPU "
+                   "path runs) per objective, K=3 objectives in parallel threads, then the reference "
+                   "combinedGraphReference + dijkstraCsrGraph") if have_ref else
+                  "oracle restatement of the reference CPU path (compute only)")
+        line = {"metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": steps,
+                "steps_requested": args.steps, "warmup": 1, "ms_per_step": round(secs * 1000, 2),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+                "data": "synthetic", "impl": "reference",
+                "config": {"workload": WORKLOAD, "n": g.n, "m": upd.m, "K": K, "changes_applied": changed,
+                           "parallelism": "CPU, one thread per objective"},
+                "cpu_baseline": {"value": round(value, 2), "unit": UNIT, "cores": K, "kind": kind,
+                                 "sample": sample + f"; full workload per step, {steps} timed step(s)"},
+                "e2e": {"value": round(value, 2), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

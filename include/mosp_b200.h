@@ -1,0 +1,307 @@
+/*
+ * mosp_b200.h - C ABI of the B200 (sm_100a) DynaMOSP update engine.
+ *
+ * Every entry point takes plain pointers and sizes and returns an int
+ * status (MOSP_OK on success). Device pointers are named d_*; host arrays
+ * are named h_* or are documented as host memory. `stream` is a
+ * cudaStream_t passed as void* (NULL = the legacy default stream).
+ *
+ * Each function names the reference interface it replaces
+ * (SMShovan/MOSP-CUDA, file:line). The C++ API of the reference
+ * (sospUpdateGpu, sospFromScratchGpu, combinedGraphSospGpu,
+ * uploadDeviceGraph, mospUpdate) is rebuilt on top of these calls by the
+ * C++ layer of this library, with the reference's declarations kept.
+ *
+ * Conventions shared with the reference:
+ *   - vertex ids and CSR offsets are int32, weights int32 in [1, INT_MAX],
+ *     distances int64, parents int32 (-1 = none);
+ *   - unreachable vertices get MOSP_DISTANCE_INF and parent -1;
+ *   - parent ties are broken by the lowest parent id (canonical trees);
+ *   - multi-objective arrays are objective-major: x[k * n + v].
+ *
+ * Calls on one workspace must not overlap; a workspace is bound to the
+ * device that was current when it was created.
+ */
+#ifndef MOSP_B200_H
+#define MOSP_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MOSP_ABI_VERSION 1
+
+/* Status codes. */
+#define MOSP_OK 0
+#define MOSP_ERR_INVALID 1     /* bad argument or malformed input */
+#define MOSP_ERR_OVERFLOW 2    /* distances do not fit the packed words */
+#define MOSP_ERR_OOM 3         /* device or pinned allocation failed */
+#define MOSP_ERR_CUDA 4        /* a CUDA runtime call failed */
+#define MOSP_ERR_TIMEOUT 5     /* a bounded device-side wait ran out */
+#define MOSP_ERR_UNSUPPORTED 6 /* device lacks a required feature */
+
+/* Distance sentinel (same value as the reference's DISTANCE_INF,
+ * headers/csrGraph.cuh:185). Values >= MOSP_DISTANCE_INF / 2 mean INF. */
+#define MOSP_DISTANCE_INF (0x7fffffffffffffffLL / 4)
+
+/* Largest number of objectives of one fused call and of the combined
+ * graph (the reference's limit, src/combinedGraphGpu.cu:259). */
+#define MOSP_MAX_OBJECTIVES 32
+
+typedef struct mosp_workspace mosp_workspace;
+
+/* Counters of one SOSP update (reference SospStats,
+ * headers/sospUpdateGpu.cuh:35-45). */
+typedef struct mosp_sosp_stats {
+  int invalidated;    /* vertices in invalidated subtrees */
+  int jump_rounds;    /* pointer-jumping rounds */
+  int iterations;     /* near-far push iterations */
+  int epochs;         /* far-pile threshold increases */
+  long long pushes;   /* vertex expansions */
+  int packed_parents; /* 1: (distance, parent) words; 0: distance-only */
+  int reserved;
+} mosp_sosp_stats;
+
+/* Counters of the combined-graph step (reference CombineStats,
+ * headers/combinedGraphGpu.cuh:17-23). */
+typedef struct mosp_combine_stats {
+  int edges;          /* edges of the combined graph */
+  int reserved;
+  long long scale;    /* L = lcm(Pref): distances are in units of 1/L */
+  long long delta;    /* near-far bucket width used for Step 3 */
+  mosp_sosp_stats search;
+} mosp_combine_stats;
+
+/* Stage times of mosp_update_host, milliseconds (reference MospTimings,
+ * headers/mospUpdate.cuh:35-46). */
+typedef struct mosp_timings {
+  double apply_batch;  /* host: apply the batch to the CSR */
+  double upload;       /* graph, trees and batch to the GPU */
+  double objectives;   /* GPU: the K SOSP updates (one fused launch) */
+  double combined;     /* GPU: combined graph + its SOSP tree */
+  double costs;        /* GPU: MOSP path costs */
+  double download;     /* results back to the host */
+} mosp_timings;
+
+/* ---------------------------------------------------------------------- */
+/* Library and helpers                                                      */
+/* ---------------------------------------------------------------------- */
+
+/* MOSP_ABI_VERSION of the loaded library. */
+int mosp_abi_version(void);
+
+/* Message of the last failing call on this host thread ("" if none). */
+const char *mosp_last_error(void);
+
+/* Short name of a status code. */
+const char *mosp_status_name(int status);
+
+/* Default near-far bucket width max(1, 32 * avgWeight / avgOutDegree).
+ * Replaces defaultDelta (src/sospUpdateGpu.cu:607-616). */
+long long mosp_default_delta(long long num_edges, int num_nodes,
+                             long long weight_sum);
+
+/* Packing of (distance, parent) words for n vertices and weights up to
+ * max_weight: *parent_bits = bits of the parent field, or 0 when the bound
+ * (n - 1) * max_weight does not fit next to it (distance-only words with
+ * parent recovery); *max_distance = that bound. MOSP_ERR_OVERFLOW if the
+ * bound does not fit in 62 bits. Replaces choosePacking / makePacking
+ * (src/sospUpdateGpu.cu:133-143, 670-681). */
+int mosp_choose_packing(int n, long long max_weight, int *parent_bits,
+                        unsigned long long *max_distance);
+
+/* L = lcm(Pref) of the combined graph, 0 if invalid (a value < 1, K values
+ * expected, or L > 2^20). h_pref may be NULL (all 1s). Replaces
+ * preferenceScale (src/combinedGraphGpu.cu:129-147). */
+long long mosp_preference_scale(const int *h_pref, int K);
+
+/* ---------------------------------------------------------------------- */
+/* Workspace (device scratch reused by every call; replaces SospWorkspace,  */
+/* headers/sospUpdateGpu.cuh:53-79, and CombineWorkspace,                   */
+/* headers/combinedGraphGpu.cuh:28-50)                                      */
+/* ---------------------------------------------------------------------- */
+
+int mosp_workspace_create(mosp_workspace **out);
+void mosp_workspace_destroy(mosp_workspace *ws);
+
+/* Reserve scratch for K objectives of graphs with up to n vertices
+ * (no-op if large enough). */
+int mosp_workspace_reserve(mosp_workspace *ws, int n, int K);
+
+/* Bound on every device-side wait of the persistent kernels (default
+ * 10000 ms). A run that exceeds it stops and returns MOSP_ERR_TIMEOUT. */
+int mosp_workspace_set_timeout_ms(mosp_workspace *ws, long long ms);
+
+/* Launch shape of the persistent kernels: CTAs per SM (0 = as many as
+ * fit). Results do not depend on it. */
+int mosp_workspace_set_ctas_per_sm(mosp_workspace *ws, int ctas_per_sm);
+
+/* Grid size (CTAs) the persistent kernels use on this device. */
+int mosp_workspace_grid(mosp_workspace *ws, int *ctas);
+
+/* Per-launch timing: when on, the engine records CUDA events around each
+ * persistent launch on the caller's stream; mosp_workspace_last_timing
+ * returns the durations (ms) of the last SOSP-update launch and the last
+ * combined-graph launch (after the call that ran them returned). */
+int mosp_workspace_enable_timing(mosp_workspace *ws, int on);
+int mosp_workspace_last_timing(mosp_workspace *ws, float *update_ms,
+                               float *combined_ms);
+
+/* Device buffer number `slot` (0..31) of the workspace, grown to at least
+ * `bytes` (contents kept only while it does not grow); freed with the
+ * workspace. Lets a caller keep its graph and trees on the device between
+ * calls without managing allocations. No counterpart in the reference. */
+int mosp_workspace_buffer(mosp_workspace *ws, int slot, unsigned long long bytes,
+                          void **d_ptr);
+
+/* ---------------------------------------------------------------------- */
+/* Device graph                                                             */
+/* ---------------------------------------------------------------------- */
+
+/* From the out-edge CSR (d_out_row[n+1], d_out_col[m]) and edge-major
+ * weights (d_edge_major_w[e*K+k]) build on the GPU the objective-major
+ * weight columns d_out_w[k*m+e] and the reverse CSR d_in_row[n+1],
+ * d_in_col[m], d_in_w[k*m+e]. Also checks that the CSR is well formed
+ * (offsets monotone from 0 to m, ids in [0, n)). Replaces the GPU part
+ * of uploadDeviceGraph (src/deviceGraph.cu:87-135). */
+int mosp_build_device_graph(mosp_workspace *ws, int n, int m, int K,
+                            const int *d_out_row, const int *d_out_col,
+                            const int *d_edge_major_w, int *d_out_w,
+                            int *d_in_row, int *d_in_col, int *d_in_w,
+                            void *stream);
+
+/* ---------------------------------------------------------------------- */
+/* SOSP update engine                                                       */
+/* ---------------------------------------------------------------------- */
+
+/* Incremental SOSP update of one objective, in place: on entry
+ * d_dist[n] / d_parent[n] hold the tree of the old graph, on return the
+ * tree of the graph whose out- and in-edges are given (with canonical
+ * input trees the result is the canonical tree). changed_from/to
+ * (n_changed entries, device) are the deleted or weight-increased edges,
+ * insert_heads (n_heads, device) the heads of all inserted edges.
+ * delta > 0 is the near-far bucket width, max_weight the largest weight.
+ * Synchronous; stats may be NULL. Replaces sospUpdateGpu
+ * (headers/sospUpdateGpu.cuh:98-102, src/sospUpdateGpu.cu:685-717). */
+int mosp_sosp_update(mosp_workspace *ws, int n, int m, const int *d_out_row,
+                     const int *d_out_col, const int *d_out_w,
+                     const int *d_in_row, const int *d_in_col,
+                     const int *d_in_w, const int *d_changed_from,
+                     const int *d_changed_to, int n_changed,
+                     const int *d_insert_heads, int n_heads, int source,
+                     long long delta, long long max_weight, long long *d_dist,
+                     int *d_parent, mosp_sosp_stats *stats, void *stream);
+
+/* The K (<= 32) SOSP updates of one MOSP update in ONE persistent launch:
+ * the objectives share the topology and the insert heads and run their
+ * near-far loops side by side behind the same grid barriers. Every
+ * h_-prefixed array has K entries in host memory; the pointers in them
+ * are device pointers. stats (K entries) may be NULL. The per-objective
+ * results equal K calls of mosp_sosp_update. Replaces the K calls of
+ * sospUpdateGpu in mospUpdate (src/mospUpdate.cu:167-194). */
+int mosp_sosp_update_multi(
+    mosp_workspace *ws, int n, int m, int K, const int *d_out_row,
+    const int *d_out_col, const int *const *h_out_w, const int *d_in_row,
+    const int *d_in_col, const int *const *h_in_w,
+    const int *const *h_changed_from, const int *const *h_changed_to,
+    const int *h_n_changed, const int *d_insert_heads, int n_heads,
+    int source, const long long *h_delta, const long long *h_max_weight,
+    long long *const *h_dist, int *const *h_parent, mosp_sosp_stats *stats,
+    void *stream);
+
+/* Canonical single-source shortest paths from scratch. Replaces
+ * sospFromScratchGpu (headers/sospUpdateGpu.cuh:107-110,
+ * src/sospUpdateGpu.cu:719-745). */
+int mosp_sosp_from_scratch(mosp_workspace *ws, int n, int m,
+                           const int *d_out_row, const int *d_out_col,
+                           const int *d_out_w, int source, long long delta,
+                           long long max_weight, long long *d_dist,
+                           int *d_parent, mosp_sosp_stats *stats,
+                           void *stream);
+
+/* Steps 2-3 of the MOSP update in one persistent launch: build the
+ * combined graph of the K trees d_parents[k*n+v] (edge (p,v) iff p is the
+ * parent of v in some tree; weight L*(K+1) - sum_{i: Parent_i[v]==p}
+ * L/Pref_i) and its canonical SSSP tree from source (distances in units
+ * of 1/L). h_pref: K host values or NULL (all 1s). delta <= 0 selects the
+ * default width of the combined graph. Replaces combinedGraphSospGpu
+ * (headers/combinedGraphGpu.cuh:65-69, src/combinedGraphGpu.cu:251-317). */
+int mosp_combined_sosp(mosp_workspace *ws, int n, int K, const int *d_parents,
+                       const int *h_pref, int source, long long delta,
+                       long long *d_dist, int *d_parent,
+                       mosp_combine_stats *stats, void *stream);
+
+/* MOSP path costs on the GPU: d_costs[v*KG+k] = objective-k length of the
+ * tree path source -> v in the graph (d_out_row, d_out_col, objective-major
+ * d_out_w with KG columns), where edge (p,v) is the first occurrence of v
+ * in row p; MOSP_DISTANCE_INF if v is unreachable. MOSP_ERR_INVALID if a
+ * tree edge is not in the graph. Replaces the host mospPathCosts
+ * (src/combinedGraphGpu.cu:161-208). */
+int mosp_path_costs(mosp_workspace *ws, int n, int m, int KG,
+                    const int *d_out_row, const int *d_out_col,
+                    const int *d_out_w, const int *d_parent, int source,
+                    long long *d_costs, void *stream);
+
+/* The device part of one MOSP update: K fused SOSP updates (as
+ * mosp_sosp_update_multi, with the objective-major weight columns
+ * d_out_w / d_in_w of K objectives starting at column 0), then Steps 2-3
+ * (mosp_combined_sosp) on the updated trees, queued back to back with one
+ * synchronization at the end. d_dist/d_parent hold the K trees
+ * (objective-major), d_changed_from/to the concatenated per-objective
+ * change lists with h_changed_offset[K+1] (host) delimiting them.
+ * Replaces the GPU stages of mospUpdate (src/mospUpdate.cu:167-209). */
+int mosp_update_device(mosp_workspace *ws, int n, int m, int K,
+                       const int *d_out_row, const int *d_out_col,
+                       const int *d_out_w, const int *d_in_row,
+                       const int *d_in_col, const int *d_in_w,
+                       const int *d_changed_from, const int *d_changed_to,
+                       const int *h_changed_offset, const int *d_insert_heads,
+                       int n_heads, int source, const long long *h_delta,
+                       const long long *h_max_weight, const int *h_pref,
+                       long long *d_dist, int *d_parent,
+                       long long *d_comb_dist, int *d_comb_parent,
+                       mosp_sosp_stats *stats, mosp_combine_stats *cstats,
+                       void *stream);
+
+/* ---------------------------------------------------------------------- */
+/* Whole MOSP update from host memory (the reference's in-memory pipeline)  */
+/* ---------------------------------------------------------------------- */
+
+/* One MOSP update with host inputs and outputs: apply the batch to the
+ * graph (n vertices, KG objectives, m edges; h_w edge-major e*KG+k),
+ * upload, run the first K objectives (K <= KG; 0 = all) and Steps 2-3 on
+ * the GPU, download, and (if h_costs != NULL) compute the MOSP path costs
+ * (n*KG) on the GPU. Inputs: inserts "u v w1..wKG" (h_ins_w insertion-
+ * major), deletes "u v", initial trees h_init_dist/h_init_parent (K*n,
+ * rooted at source). h_pref: K values or NULL; delta <= 0: default per
+ * objective. Outputs: h_dist/h_parent (K*n), h_comb_dist/h_comb_parent
+ * (n). timings may be NULL. Replaces mospUpdate
+ * (headers/mospUpdate.cuh:69-73, src/mospUpdate.cu:57-225). */
+int mosp_update_host(mosp_workspace *ws, int n, int KG, int m,
+                     const int *h_row, const int *h_col, const int *h_w,
+                     int n_ins, const int *h_ins_from, const int *h_ins_to,
+                     const int *h_ins_w, int n_del, const int *h_del_from,
+                     const int *h_del_to, const long long *h_init_dist,
+                     const int *h_init_parent, int K, int source,
+                     const int *h_pref, long long delta, long long *h_dist,
+                     int *h_parent, long long *h_comb_dist,
+                     int *h_comb_parent, long long *h_costs,
+                     mosp_timings *timings);
+
+/* ---------------------------------------------------------------------- */
+/* Failure-path check                                                       */
+/* ---------------------------------------------------------------------- */
+
+/* Runs a grid barrier that one CTA never reaches, bounded by timeout_ms
+ * (<= 10000); *device_status receives the status the kernel reported
+ * (MOSP_ERR_TIMEOUT when the bounded wait works). The workspace stays
+ * usable afterwards. No counterpart in the reference (whose grid barriers
+ * are unbounded, src/sospUpdateGpu.cu:644-649). */
+int mosp_debug_barrier_timeout(mosp_workspace *ws, long long timeout_ms,
+                               int *device_status);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MOSP_B200_H */

@@ -1,0 +1,891 @@
+// capi.cu - the C ABI of the engine (include/mosp_b200.h): workspace
+// management, argument checks, packing choice, launches and the readback
+// of the device control blocks.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <string>
+
+#include "engine.h"
+#include "mosp_b200.h"
+
+using namespace mospb200;
+
+// ---------------------------------------------------------------------------
+// Errors
+// ---------------------------------------------------------------------------
+namespace {
+thread_local std::string g_lastError;
+
+int fail(int status, const std::string &message) {
+  g_lastError = message;
+  return status;
+}
+
+int cudaFail(cudaError_t err, const char *what) {
+  return fail(MOSP_ERR_CUDA, std::string("CUDA error: ") + cudaGetErrorString(err) + " (" +
+                                 what + ")");
+}
+
+#define MOSP_CUDA(call)                                   \
+  do {                                                    \
+    cudaError_t err_ = (call);                            \
+    if (err_ != cudaSuccess) return cudaFail(err_, #call); \
+  } while (0)
+
+constexpr int kControlBlocks = 4;  // 0: update/scratch, 1: combined, 2: build, 3: costs
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Workspace
+// ---------------------------------------------------------------------------
+struct mosp_workspace {
+  int device = -1;
+  long long timeoutNs = 10000LL * 1000000LL;
+  int ctasPerSm = 0;
+  bool shapeValid = false;
+  LaunchShape shape{};
+  // engine lists: kCap objectives x nCap vertices
+  long long nCap = 0;
+  int kCap = 0;
+  u64 *packed = nullptr;
+  int *val = nullptr, *stamp = nullptr, *inFar = nullptr, *cand = nullptr;
+  int *near0 = nullptr, *near1 = nullptr, *far0 = nullptr, *far1 = nullptr;
+  int *gen = nullptr;  // device stamp generation
+  bool dirty = false;  // an aborted run may have left inFar/stamp set
+  // control blocks
+  EngineControl *ctl = nullptr;
+  EngineControl *hostCtl = nullptr;  // pinned
+  long long *blockSums = nullptr;
+  int blockSumsCap = 0;
+  // combined graph
+  long long combN = 0, combEdgesCap = 0;
+  int *combDeg = nullptr, *combRow = nullptr, *combCol = nullptr, *combW = nullptr;
+  // reverse-CSR build cursor
+  long long cursorCap = 0;
+  int *cursor = nullptr;
+  // path costs
+  long long costN = 0;
+  int costKG = 0;
+  int *edgeOf = nullptr, *anc0 = nullptr, *anc1 = nullptr;
+  long long *acc0 = nullptr, *acc1 = nullptr;
+  // per-launch timing (mosp_workspace_enable_timing)
+  bool timing = false;
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  float lastUpdateMs = 0, lastCombinedMs = 0;
+  // caller buffers (mosp_workspace_buffer)
+  void *user[32] = {nullptr};
+  unsigned long long userBytes[32] = {0};
+};
+
+namespace {
+
+template <typename T>
+int deviceAlloc(T **ptr, size_t count) {
+  if (*ptr != nullptr) cudaFree(*ptr);
+  *ptr = nullptr;
+  cudaError_t err = cudaMalloc(reinterpret_cast<void **>(ptr), std::max<size_t>(count, 1) * sizeof(T));
+  if (err != cudaSuccess) {
+    cudaGetLastError();
+    *ptr = nullptr;
+    return fail(MOSP_ERR_OOM, std::string("device allocation of ") +
+                                  std::to_string(count * sizeof(T)) + " bytes failed: " +
+                                  cudaGetErrorString(err));
+  }
+  return MOSP_OK;
+}
+
+void releaseLists(mosp_workspace *ws) {
+  for (void *p : {static_cast<void *>(ws->packed), static_cast<void *>(ws->val),
+                  static_cast<void *>(ws->stamp), static_cast<void *>(ws->inFar),
+                  static_cast<void *>(ws->cand), static_cast<void *>(ws->near0),
+                  static_cast<void *>(ws->near1), static_cast<void *>(ws->far0),
+                  static_cast<void *>(ws->far1)}) {
+    if (p) cudaFree(p);
+  }
+  ws->packed = nullptr;
+  ws->val = ws->stamp = ws->inFar = ws->cand = nullptr;
+  ws->near0 = ws->near1 = ws->far0 = ws->far1 = nullptr;
+  ws->nCap = 0;
+  ws->kCap = 0;
+}
+
+int ensureShape(mosp_workspace *ws) {
+  if (ws->shapeValid) return MOSP_OK;
+  MOSP_CUDA(cudaSetDevice(ws->device));
+  cudaError_t err = queryLaunchShape(ws->ctasPerSm, ws->shape);
+  if (err == cudaErrorNotSupported) {
+    return fail(MOSP_ERR_UNSUPPORTED, "the GPU does not support cooperative launches");
+  }
+  if (err != cudaSuccess) return cudaFail(err, "occupancy query");
+  const int maxCtas = std::max({ws->shape.engineCtas, ws->shape.buildCtas, ws->shape.costCtas});
+  if (maxCtas > ws->blockSumsCap) {
+    int st = deviceAlloc(&ws->blockSums, maxCtas);
+    if (st != MOSP_OK) return st;
+    ws->blockSumsCap = maxCtas;
+  }
+  ws->shapeValid = true;
+  return MOSP_OK;
+}
+
+int reserveLists(mosp_workspace *ws, long long n, int K) {
+  if (n <= ws->nCap && K <= ws->kCap) return MOSP_OK;
+  const long long newN = std::max(n, ws->nCap);
+  const int newK = std::max(K, ws->kCap);
+  releaseLists(ws);
+  const size_t total = static_cast<size_t>(newN) * newK;
+  int st = MOSP_OK;
+  if ((st = deviceAlloc(&ws->packed, total)) != MOSP_OK) return st;
+  for (int **p : {&ws->val, &ws->stamp, &ws->inFar, &ws->cand, &ws->near0, &ws->near1,
+                  &ws->far0, &ws->far1}) {
+    if ((st = deviceAlloc(p, total)) != MOSP_OK) {
+      releaseLists(ws);
+      return st;
+    }
+  }
+  MOSP_CUDA(cudaMemset(ws->stamp, 0, total * sizeof(int)));
+  MOSP_CUDA(cudaMemset(ws->inFar, 0, total * sizeof(int)));
+  MOSP_CUDA(cudaMemset(ws->gen, 0, sizeof(int)));
+  ws->nCap = newN;
+  ws->kCap = newK;
+  ws->dirty = false;
+  return MOSP_OK;
+}
+
+/// Clear the dedup state after an aborted run, or before the stamp
+/// generation could overflow.
+int cleanLists(mosp_workspace *ws, cudaStream_t s) {
+  const size_t total = static_cast<size_t>(ws->nCap) * ws->kCap;
+  if (ws->dirty) {
+    MOSP_CUDA(cudaMemsetAsync(ws->inFar, 0, total * sizeof(int), s));
+    MOSP_CUDA(cudaMemsetAsync(ws->stamp, 0, total * sizeof(int), s));
+    MOSP_CUDA(cudaMemsetAsync(ws->gen, 0, sizeof(int), s));
+    ws->dirty = false;
+  }
+  return MOSP_OK;
+}
+
+/// After a synchronous run: restart the generations well before they wrap.
+int maybeResetGenerations(mosp_workspace *ws, int finalGen, cudaStream_t s) {
+  if (finalGen > INT_MAX / 2) {
+    const size_t total = static_cast<size_t>(ws->nCap) * ws->kCap;
+    MOSP_CUDA(cudaMemsetAsync(ws->stamp, 0, total * sizeof(int), s));
+    MOSP_CUDA(cudaMemsetAsync(ws->gen, 0, sizeof(int), s));
+    MOSP_CUDA(cudaStreamSynchronize(s));
+  }
+  return MOSP_OK;
+}
+
+int reserveCombined(mosp_workspace *ws, long long n, int K) {
+  int st = MOSP_OK;
+  if (n > ws->combN) {
+    if ((st = deviceAlloc(&ws->combDeg, n + 1)) != MOSP_OK) return st;
+    if ((st = deviceAlloc(&ws->combRow, n + 1)) != MOSP_OK) return st;
+    ws->combN = n;
+  }
+  const long long edges = n * K;
+  if (edges > ws->combEdgesCap) {
+    if ((st = deviceAlloc(&ws->combCol, edges)) != MOSP_OK) return st;
+    if ((st = deviceAlloc(&ws->combW, edges)) != MOSP_OK) return st;
+    ws->combEdgesCap = edges;
+  }
+  return MOSP_OK;
+}
+
+cudaStream_t asStream(void *s) { return static_cast<cudaStream_t>(s); }
+
+/// Bits of the parent field and the distance bound (reference
+/// src/sospUpdateGpu.cu:133-143, 670-681).
+int choosePacking(long long n, long long maxWeight, int &bits, u64 &maxDist) {
+  const u64 outputMax = static_cast<u64>(MOSP_DISTANCE_INF / 2 - 1);
+  const u64 weight = static_cast<u64>(std::max(maxWeight, 1LL));
+  const u64 hops = static_cast<u64>(std::max(n - 1, 1LL));
+  if (weight > outputMax / hops) {
+    return fail(MOSP_ERR_OVERFLOW, "Error: distances up to " + std::to_string(weight) + " * " +
+                                       std::to_string(hops) + " do not fit in 62 bits.");
+  }
+  maxDist = weight * hops;
+  int b = 1;
+  while ((1ULL << b) - 1 < static_cast<u64>(n)) ++b;
+  const u64 storable = (kInfWord >> b) - 1;
+  bits = maxDist <= storable ? b : 0;
+  return MOSP_OK;
+}
+
+void setObjective(ObjectiveArgs &o, int bits, u64 maxDist, long long delta) {
+  o.parentBits = bits;
+  o.noParent = bits > 0 ? ((1ULL << bits) - 1) : 0;
+  o.maxDist = maxDist;
+  o.delta = static_cast<u64>(delta);
+}
+
+void fillLists(EngineParams &p, mosp_workspace *ws, int block) {
+  p.timeoutNs = ws->timeoutNs;
+  p.genPtr = ws->gen;
+  p.packed = ws->packed;
+  p.val = ws->val;
+  p.stamp = ws->stamp;
+  p.inFar = ws->inFar;
+  p.cand = ws->cand;
+  p.nearL0 = ws->near0;
+  p.nearL1 = ws->near1;
+  p.farL0 = ws->far0;
+  p.farL1 = ws->far1;
+  p.stride = ws->nCap;
+  p.ctl = ws->ctl + block;
+  p.blockSums = ws->blockSums;
+}
+
+int maxRoundsFor(long long n) {
+  int rounds = 0;
+  while ((1LL << rounds) < n) ++rounds;
+  return rounds + 1;
+}
+
+int markEvent(mosp_workspace *ws, int i, cudaStream_t s) {
+  if (!ws->timing) return MOSP_OK;
+  if (ws->ev[i] == nullptr) MOSP_CUDA(cudaEventCreate(&ws->ev[i]));
+  MOSP_CUDA(cudaEventRecord(ws->ev[i], s));
+  return MOSP_OK;
+}
+
+/// Durations between the recorded events (after the stream was synced).
+void readEvents(mosp_workspace *ws, float *first, float *second) {
+  if (!ws->timing) return;
+  if (first != nullptr) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, ws->ev[0], ws->ev[1]) == cudaSuccess) *first = ms;
+  }
+  if (second != nullptr) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, ws->ev[1], ws->ev[2]) == cudaSuccess) *second = ms;
+  }
+}
+
+/// Queue one engine launch (control block `block` is cleared first).
+int queueEngine(mosp_workspace *ws, const EngineParams &p, int block, cudaStream_t s) {
+  MOSP_CUDA(cudaMemsetAsync(ws->ctl + block, 0, sizeof(EngineControl), s));
+  MOSP_CUDA(launchEngine(p, ws->shape.engineCtas, s));
+  return MOSP_OK;
+}
+
+/// Copy control blocks [first, first + count) to the host and wait.
+int readControl(mosp_workspace *ws, int first, int count, cudaStream_t s) {
+  MOSP_CUDA(cudaMemcpyAsync(ws->hostCtl + first, ws->ctl + first, count * sizeof(EngineControl),
+                            cudaMemcpyDeviceToHost, s));
+  cudaError_t err = cudaStreamSynchronize(s);
+  if (err != cudaSuccess) return cudaFail(err, "engine run");
+  return MOSP_OK;
+}
+
+/// Device-side status of a finished run.
+int controlStatus(mosp_workspace *ws, const EngineControl &c) {
+  if (c.status != 0) {
+    ws->dirty = true;
+    return fail(MOSP_ERR_TIMEOUT,
+                "Error: a device-side wait of the persistent kernel exceeded its limit; the run "
+                "was stopped.");
+  }
+  if (c.invalid) {
+    ws->dirty = true;
+    return fail(MOSP_ERR_INVALID,
+                "Error: malformed input (a vertex id, parent or change endpoint out of range, a "
+                "cycle in the parent array, or a tree edge missing from the graph).");
+  }
+  if (c.overflow) {
+    return fail(MOSP_ERR_OVERFLOW,
+                "Error: an input distance is negative or larger than (n - 1) * maxWeight; the "
+                "initial tree does not belong to this graph.");
+  }
+  return MOSP_OK;
+}
+
+void fillStats(const EngineControl &c, int k, int bits, mosp_sosp_stats *s) {
+  s->invalidated = c.invalidated[k];
+  s->jump_rounds = c.rounds;
+  s->iterations = c.iterations[k];
+  s->epochs = c.epochs[k];
+  s->pushes = c.pushes[k];
+  s->packed_parents = bits > 0 ? 1 : 0;
+  s->reserved = 0;
+}
+
+int checkWorkspace(mosp_workspace *ws) {
+  if (ws == nullptr) return fail(MOSP_ERR_INVALID, "null workspace");
+  int dev = -1;
+  MOSP_CUDA(cudaGetDevice(&dev));
+  if (dev != ws->device) MOSP_CUDA(cudaSetDevice(ws->device));
+  return ensureShape(ws);
+}
+
+struct UpdateArgs {
+  int n, m, K;
+  const int *outRow, *outCol, *inRow, *inCol;
+  const int *const *outW;
+  const int *const *inW;
+  const int *const *chFrom;
+  const int *const *chTo;
+  const int *nChanged;
+  const int *heads;
+  int nHeads, source;
+  const long long *delta;
+  const long long *maxWeight;
+  long long *const *dist;
+  int *const *parent;
+};
+
+/// Build the parameters of a fused K-objective update.
+int prepareUpdate(mosp_workspace *ws, const UpdateArgs &a, EngineParams &p, int *bitsOut) {
+  if (a.n <= 0 || a.m < 0 || a.K < 1 || a.K > kMaxK || a.source < 0 || a.source >= a.n ||
+      a.nHeads < 0 || (a.nHeads > 0 && a.heads == nullptr) || a.outRow == nullptr ||
+      a.inRow == nullptr || (a.m > 0 && (a.outCol == nullptr || a.inCol == nullptr))) {
+    return fail(MOSP_ERR_INVALID, "Error: invalid SOSP update arguments.");
+  }
+  int st = reserveLists(ws, a.n, a.K);
+  if (st != MOSP_OK) return st;
+  std::memset(&p, 0, sizeof(p));
+  p.n = a.n;
+  p.m = a.m;
+  p.K = a.K;
+  p.source = a.source;
+  p.mode = kModeUpdate;
+  p.maxRounds = maxRoundsFor(a.n);
+  p.nHeads = a.nHeads;
+  p.outRow = a.outRow;
+  p.outCol = a.outCol;
+  p.inRow = a.inRow;
+  p.inCol = a.inCol;
+  p.heads = a.heads;
+  for (int k = 0; k < a.K; ++k) {
+    if (a.delta[k] <= 0) return fail(MOSP_ERR_INVALID, "Error: delta must be positive.");
+    if (a.nChanged[k] < 0 || (a.nChanged[k] > 0 && (a.chFrom[k] == nullptr || a.chTo[k] == nullptr)) ||
+        a.dist[k] == nullptr || a.parent[k] == nullptr || (a.m > 0 && (a.outW[k] == nullptr || a.inW[k] == nullptr))) {
+      return fail(MOSP_ERR_INVALID, "Error: invalid SOSP update arguments.");
+    }
+    int bits = 0;
+    u64 maxDist = 0;
+    if ((st = choosePacking(a.n, a.maxWeight[k], bits, maxDist)) != MOSP_OK) return st;
+    ObjectiveArgs &o = p.obj[k];
+    o.outW = a.outW[k];
+    o.inW = a.inW[k];
+    o.dist = a.dist[k];
+    o.parent = a.parent[k];
+    o.chFrom = a.chFrom[k];
+    o.chTo = a.chTo[k];
+    o.nChanged = a.nChanged[k];
+    setObjective(o, bits, maxDist, a.delta[k]);
+    bitsOut[k] = bits;
+  }
+  return MOSP_OK;
+}
+
+/// Build the parameters of the combined-graph step.
+int prepareCombined(mosp_workspace *ws, int n, int K, const int *d_parents, const int *h_pref,
+                    int source, long long delta, long long *d_dist, int *d_parent,
+                    EngineParams &p, long long &scale, int &bits) {
+  if (K <= 0 || K > 32 || n <= 0 || source < 0 || source >= n || d_parents == nullptr ||
+      d_dist == nullptr || d_parent == nullptr) {
+    return fail(MOSP_ERR_INVALID, "Error: invalid combined-graph parameters.");
+  }
+  scale = mosp_preference_scale(h_pref, K);
+  if (scale == 0) {
+    return fail(MOSP_ERR_INVALID, "Error: invalid preference vector (need K values >= 1).");
+  }
+  int st = reserveLists(ws, n, 1);
+  if (st != MOSP_OK) return st;
+  if ((st = reserveCombined(ws, n, K)) != MOSP_OK) return st;
+  std::memset(&p, 0, sizeof(p));
+  p.n = n;
+  p.K = 1;
+  p.source = source;
+  p.mode = kModeCombined;
+  p.combParents = d_parents;
+  p.combDeg = ws->combDeg;
+  p.combRow = ws->combRow;
+  p.combCol = ws->combCol;
+  p.combW = ws->combW;
+  p.combK = K;
+  p.combBase = static_cast<int>(scale * (K + 1));
+  p.combDelta = delta;
+  for (int k = 0; k < K; ++k) {
+    p.prefTerms[k] = static_cast<int>(h_pref == nullptr ? scale : scale / h_pref[k]);
+  }
+  u64 maxDist = 0;
+  if ((st = choosePacking(n, p.combBase, bits, maxDist)) != MOSP_OK) return st;
+  ObjectiveArgs &o = p.obj[0];
+  o.dist = d_dist;
+  o.parent = d_parent;
+  setObjective(o, bits, maxDist, delta > 0 ? delta : 1);
+  return MOSP_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// extern "C"
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int mosp_abi_version(void) { return MOSP_ABI_VERSION; }
+
+const char *mosp_last_error(void) { return g_lastError.c_str(); }
+
+const char *mosp_status_name(int status) {
+  switch (status) {
+    case MOSP_OK: return "MOSP_OK";
+    case MOSP_ERR_INVALID: return "MOSP_ERR_INVALID";
+    case MOSP_ERR_OVERFLOW: return "MOSP_ERR_OVERFLOW";
+    case MOSP_ERR_OOM: return "MOSP_ERR_OOM";
+    case MOSP_ERR_CUDA: return "MOSP_ERR_CUDA";
+    case MOSP_ERR_TIMEOUT: return "MOSP_ERR_TIMEOUT";
+    case MOSP_ERR_UNSUPPORTED: return "MOSP_ERR_UNSUPPORTED";
+    default: return "MOSP_ERR_UNKNOWN";
+  }
+}
+
+long long mosp_default_delta(long long num_edges, int num_nodes, long long weight_sum) {
+  if (num_edges <= 0 || num_nodes <= 0) return 1;
+  // 32 * (average weight) / (average out-degree); only the speed depends on it
+  const double averageWeight = static_cast<double>(weight_sum) / num_edges;
+  const double averageDegree = static_cast<double>(num_edges) / num_nodes;
+  return std::max(1LL, static_cast<long long>(32.0 * averageWeight / averageDegree));
+}
+
+int mosp_choose_packing(int n, long long max_weight, int *parent_bits,
+                        unsigned long long *max_distance) {
+  int bits = 0;
+  u64 maxDist = 0;
+  const int st = choosePacking(std::max(n, 1), max_weight, bits, maxDist);
+  if (st != MOSP_OK) return st;
+  if (parent_bits) *parent_bits = bits;
+  if (max_distance) *max_distance = maxDist;
+  return MOSP_OK;
+}
+
+long long mosp_preference_scale(const int *h_pref, int K) {
+  // L = lcm(Pref) <= 2^20 (reference src/combinedGraphGpu.cu:129-147)
+  if (h_pref == nullptr) return 1;
+  if (K <= 0) return 0;
+  long long scale = 1;
+  for (int i = 0; i < K; ++i) {
+    if (h_pref[i] < 1) return 0;
+    scale = scale / std::gcd(scale, static_cast<long long>(h_pref[i])) * h_pref[i];
+    if (scale > (1LL << 20)) return 0;
+  }
+  return scale;
+}
+
+int mosp_workspace_create(mosp_workspace **out) {
+  if (out == nullptr) return fail(MOSP_ERR_INVALID, "null output pointer");
+  *out = nullptr;
+  mosp_workspace *ws = new mosp_workspace();
+  MOSP_CUDA(cudaGetDevice(&ws->device));
+  int st = deviceAlloc(&ws->ctl, kControlBlocks);
+  if (st == MOSP_OK) st = deviceAlloc(&ws->gen, 1);
+  if (st == MOSP_OK && cudaMemset(ws->gen, 0, sizeof(int)) != cudaSuccess) st = MOSP_ERR_CUDA;
+  if (st == MOSP_OK &&
+      cudaMallocHost(reinterpret_cast<void **>(&ws->hostCtl), kControlBlocks * sizeof(EngineControl)) !=
+          cudaSuccess) {
+    st = fail(MOSP_ERR_OOM, "pinned allocation failed");
+  }
+  if (st != MOSP_OK) {
+    mosp_workspace_destroy(ws);
+    return st;
+  }
+  *out = ws;
+  return MOSP_OK;
+}
+
+void mosp_workspace_destroy(mosp_workspace *ws) {
+  if (ws == nullptr) return;
+  int dev = -1;
+  cudaGetDevice(&dev);
+  if (ws->device >= 0) cudaSetDevice(ws->device);
+  releaseLists(ws);
+  for (void *p : {static_cast<void *>(ws->ctl), static_cast<void *>(ws->gen),
+                  static_cast<void *>(ws->blockSums), static_cast<void *>(ws->combDeg),
+                  static_cast<void *>(ws->combRow), static_cast<void *>(ws->combCol),
+                  static_cast<void *>(ws->combW), static_cast<void *>(ws->cursor),
+                  static_cast<void *>(ws->edgeOf), static_cast<void *>(ws->anc0),
+                  static_cast<void *>(ws->anc1), static_cast<void *>(ws->acc0),
+                  static_cast<void *>(ws->acc1)}) {
+    if (p) cudaFree(p);
+  }
+  for (void *p : ws->user) {
+    if (p) cudaFree(p);
+  }
+  for (cudaEvent_t e : ws->ev) {
+    if (e) cudaEventDestroy(e);
+  }
+  if (ws->hostCtl) cudaFreeHost(ws->hostCtl);
+  if (dev >= 0) cudaSetDevice(dev);
+  delete ws;
+}
+
+int mosp_workspace_reserve(mosp_workspace *ws, int n, int K) {
+  int st = checkWorkspace(ws);
+  if (st != MOSP_OK) return st;
+  if (n < 0 || K < 1 || K > kMaxK) return fail(MOSP_ERR_INVALID, "invalid reserve size");
+  if ((st = reserveLists(ws, std::max(n, 1), K)) != MOSP_OK) return st;
+  return reserveCombined(ws, std::max(n, 1), K);
+}
+
+int mosp_workspace_set_timeout_ms(mosp_workspace *ws, long long ms) {
+  if (ws == nullptr || ms <= 0) return fail(MOSP_ERR_INVALID, "invalid timeout");
+  ws->timeoutNs = ms * 1000000LL;
+  return MOSP_OK;
+}
+
+int mosp_workspace_set_ctas_per_sm(mosp_workspace *ws, int ctas_per_sm) {
+  if (ws == nullptr || ctas_per_sm < 0) return fail(MOSP_ERR_INVALID, "invalid launch shape");
+  ws->ctasPerSm = ctas_per_sm;
+  ws->shapeValid = false;
+  return MOSP_OK;
+}
+
+int mosp_workspace_buffer(mosp_workspace *ws, int slot, unsigned long long bytes, void **d_ptr) {
+  int st = checkWorkspace(ws);
+  if (st != MOSP_OK) return st;
+  if (slot < 0 || slot >= 32 || d_ptr == nullptr) return fail(MOSP_ERR_INVALID, "invalid buffer slot");
+  if (bytes > ws->userBytes[slot] || ws->user[slot] == nullptr) {
+    char *p = static_cast<char *>(ws->user[slot]);
+    const unsigned long long grow = std::max(bytes, ws->userBytes[slot] + ws->userBytes[slot] / 8);
+    if ((st = deviceAlloc(&p, grow)) != MOSP_OK) {
+      ws->user[slot] = nullptr;
+      ws->userBytes[slot] = 0;
+      return st;
+    }
+    ws->user[slot] = p;
+    ws->userBytes[slot] = grow;
+  }
+  *d_ptr = ws->user[slot];
+  return MOSP_OK;
+}
+
+int mosp_workspace_enable_timing(mosp_workspace *ws, int on) {
+  if (ws == nullptr) return fail(MOSP_ERR_INVALID, "null workspace");
+  ws->timing = on != 0;
+  return MOSP_OK;
+}
+
+int mosp_workspace_last_timing(mosp_workspace *ws, float *update_ms, float *combined_ms) {
+  if (ws == nullptr) return fail(MOSP_ERR_INVALID, "null workspace");
+  if (update_ms) *update_ms = ws->lastUpdateMs;
+  if (combined_ms) *combined_ms = ws->lastCombinedMs;
+  return MOSP_OK;
+}
+
+int mosp_workspace_grid(mosp_workspace *ws, int *ctas) {
+  int st = checkWorkspace(ws);
+  if (st != MOSP_OK) return st;
+  if (ctas) *ctas = ws->shape.engineCtas;
+  return MOSP_OK;
+}
+
+int mosp_build_device_graph(mosp_workspace *ws, int n, int m, int K, const int *d_out_row,
+                            const int *d_out_col, const int *d_edge_major_w, int *d_out_w,
+                            int *d_in_row, int *d_in_col, int *d_in_w, void *stream) {
+  int st = checkWorkspace(ws);
+  if (st != MOSP_OK) return st;
+  if (n <= 0 || m < 0 || K < 1 || d_out_row == nullptr || d_in_row == nullptr ||
+      (m > 0 && (d_out_col == nullptr || d_edge_major_w == nullptr || d_out_w == nullptr ||
+                 d_in_col == nullptr || d_in_w == nullptr))) {
+    return fail(MOSP_ERR_INVALID, "Error: invalid device graph arguments.");
+  }
+  if (n + 1 > ws->cursorCap) {
+    if ((st = deviceAlloc(&ws->cursor, static_cast<size_t>(n) + 1)) != MOSP_OK) return st;
+    ws->cursorCap = static_cast<long long>(n) + 1;
+  }
+  cudaStream_t s = asStream(stream);
+  BuildParams b{};
+  b.n = n;
+  b.m = m;
+  b.K = K;
+  b.timeoutNs = ws->timeoutNs;
+  b.outRow = d_out_row;
+  b.outCol = d_out_col;
+  b.edgeMajorW = d_edge_major_w;
+  b.outW = d_out_w;
+  b.inRow = d_in_row;
+  b.inCol = d_in_col;
+  b.inW = d_in_w;
+  b.cursor = ws->cursor;
+  b.blockSums = ws->blockSums;
+  b.ctl = ws->ctl + 2;
+  MOSP_CUDA(cudaMemsetAsync(ws->ctl + 2, 0, sizeof(EngineControl), s));
+  MOSP_CUDA(launchBuild(b, ws->shape.buildCtas, s));
+  if ((st = readControl(ws, 2, 1, s)) != MOSP_OK) return st;
+  const EngineControl &c = ws->hostCtl[2];
+  if (c.status != 0) return fail(MOSP_ERR_TIMEOUT, "Error: device graph build timed out.");
+  if (c.invalid) {
+    return fail(MOSP_ERR_INVALID,
+                "Error: malformed CSR (row offsets not monotone from 0 to m, or a column index "
+                "outside [0, n)).");
+  }
+  return MOSP_OK;
+}
+
+int mosp_sosp_update_multi(mosp_workspace *ws, int n, int m, int K, const int *d_out_row,
+                           const int *d_out_col, const int *const *h_out_w, const int *d_in_row,
+                           const int *d_in_col, const int *const *h_in_w,
+                           const int *const *h_changed_from, const int *const *h_changed_to,
+                           const int *h_n_changed, const int *d_insert_heads, int n_heads,
+                           int source, const long long *h_delta, const long long *h_max_weight,
+                           long long *const *h_dist, int *const *h_parent,
+                           mosp_sosp_stats *stats, void *stream) {
+  int st = checkWorkspace(ws);
+  if (st != MOSP_OK) return st;
+  if (K < 1 || K > kMaxK || h_out_w == nullptr || h_in_w == nullptr || h_changed_from == nullptr ||
+      h_changed_to == nullptr || h_n_changed == nullptr || h_delta == nullptr ||
+      h_max_weight == nullptr || h_dist == nullptr || h_parent == nullptr) {
+    return fail(MOSP_ERR_INVALID, "Error: invalid SOSP update arguments.");
+  }
+  UpdateArgs a{n,        m,           K,          d_out_row,      d_out_col,  d_in_row,
+               d_in_col, h_out_w,     h_in_w,     h_changed_from, h_changed_to, h_n_changed,
+               d_insert_heads, n_heads, source,   h_delta,        h_max_weight, h_dist,
+               h_parent};
+  EngineParams p;
+  int bits[kMaxK] = {0};
+  if ((st = prepareUpdate(ws, a, p, bits)) != MOSP_OK) return st;
+  cudaStream_t s = asStream(stream);
+  if ((st = cleanLists(ws, s)) != MOSP_OK) return st;
+  fillLists(p, ws, 0);
+  if ((st = markEvent(ws, 0, s)) != MOSP_OK) return st;
+  if ((st = queueEngine(ws, p, 0, s)) != MOSP_OK) return st;
+  if ((st = markEvent(ws, 1, s)) != MOSP_OK) return st;
+  if ((st = readControl(ws, 0, 1, s)) != MOSP_OK) return st;
+  readEvents(ws, &ws->lastUpdateMs, nullptr);
+  const EngineControl &c = ws->hostCtl[0];
+  if ((st = controlStatus(ws, c)) != MOSP_OK) return st;
+  if (stats) {
+    for (int k = 0; k < K; ++k) fillStats(c, k, bits[k], stats + k);
+  }
+  return maybeResetGenerations(ws, c.finalGen, s);
+}
+
+int mosp_sosp_update(mosp_workspace *ws, int n, int m, const int *d_out_row, const int *d_out_col,
+                     const int *d_out_w, const int *d_in_row, const int *d_in_col,
+                     const int *d_in_w, const int *d_changed_from, const int *d_changed_to,
+                     int n_changed, const int *d_insert_heads, int n_heads, int source,
+                     long long delta, long long max_weight, long long *d_dist, int *d_parent,
+                     mosp_sosp_stats *stats, void *stream) {
+  return mosp_sosp_update_multi(ws, n, m, 1, d_out_row, d_out_col, &d_out_w, d_in_row, d_in_col,
+                                &d_in_w, &d_changed_from, &d_changed_to, &n_changed,
+                                d_insert_heads, n_heads, source, &delta, &max_weight, &d_dist,
+                                &d_parent, stats, stream);
+}
+
+int mosp_sosp_from_scratch(mosp_workspace *ws, int n, int m, const int *d_out_row,
+                           const int *d_out_col, const int *d_out_w, int source, long long delta,
+                           long long max_weight, long long *d_dist, int *d_parent,
+                           mosp_sosp_stats *stats, void *stream) {
+  int st = checkWorkspace(ws);
+  if (st != MOSP_OK) return st;
+  if (n <= 0 || m < 0 || source < 0 || source >= n || delta <= 0 || d_out_row == nullptr ||
+      (m > 0 && (d_out_col == nullptr || d_out_w == nullptr)) || d_dist == nullptr ||
+      d_parent == nullptr) {
+    return fail(MOSP_ERR_INVALID, "Error: invalid SSSP arguments.");
+  }
+  if ((st = reserveLists(ws, n, 1)) != MOSP_OK) return st;
+  int bits = 0;
+  u64 maxDist = 0;
+  if ((st = choosePacking(n, max_weight, bits, maxDist)) != MOSP_OK) return st;
+  EngineParams p;
+  std::memset(&p, 0, sizeof(p));
+  p.n = n;
+  p.m = m;
+  p.K = 1;
+  p.source = source;
+  p.mode = kModeScratch;
+  p.outRow = d_out_row;
+  p.outCol = d_out_col;
+  p.obj[0].outW = d_out_w;
+  p.obj[0].dist = d_dist;
+  p.obj[0].parent = d_parent;
+  setObjective(p.obj[0], bits, maxDist, delta);
+  cudaStream_t s = asStream(stream);
+  if ((st = cleanLists(ws, s)) != MOSP_OK) return st;
+  fillLists(p, ws, 0);
+  if ((st = queueEngine(ws, p, 0, s)) != MOSP_OK) return st;
+  if ((st = readControl(ws, 0, 1, s)) != MOSP_OK) return st;
+  const EngineControl &c = ws->hostCtl[0];
+  if ((st = controlStatus(ws, c)) != MOSP_OK) return st;
+  if (stats) fillStats(c, 0, bits, stats);
+  return maybeResetGenerations(ws, c.finalGen, s);
+}
+
+int mosp_combined_sosp(mosp_workspace *ws, int n, int K, const int *d_parents, const int *h_pref,
+                       int source, long long delta, long long *d_dist, int *d_parent,
+                       mosp_combine_stats *stats, void *stream) {
+  int st = checkWorkspace(ws);
+  if (st != MOSP_OK) return st;
+  EngineParams p;
+  long long scale = 0;
+  int bits = 0;
+  if ((st = prepareCombined(ws, n, K, d_parents, h_pref, source, delta, d_dist, d_parent, p,
+                            scale, bits)) != MOSP_OK) {
+    return st;
+  }
+  cudaStream_t s = asStream(stream);
+  if ((st = cleanLists(ws, s)) != MOSP_OK) return st;
+  fillLists(p, ws, 1);
+  if ((st = markEvent(ws, 1, s)) != MOSP_OK) return st;
+  if ((st = queueEngine(ws, p, 1, s)) != MOSP_OK) return st;
+  if ((st = markEvent(ws, 2, s)) != MOSP_OK) return st;
+  if ((st = readControl(ws, 1, 1, s)) != MOSP_OK) return st;
+  readEvents(ws, nullptr, &ws->lastCombinedMs);
+  const EngineControl &c = ws->hostCtl[1];
+  if ((st = controlStatus(ws, c)) != MOSP_OK) return st;
+  if (stats) {
+    stats->edges = static_cast<int>(c.sums[0]);
+    stats->reserved = 0;
+    stats->scale = scale;
+    stats->delta = delta > 0 ? delta
+                             : mosp_default_delta(static_cast<long long>(c.sums[0]), n,
+                                                  static_cast<long long>(c.sums[1]));
+    fillStats(c, 0, bits, &stats->search);
+  }
+  return maybeResetGenerations(ws, c.finalGen, s);
+}
+
+int mosp_update_device(mosp_workspace *ws, int n, int m, int K, const int *d_out_row,
+                       const int *d_out_col, const int *d_out_w, const int *d_in_row,
+                       const int *d_in_col, const int *d_in_w, const int *d_changed_from,
+                       const int *d_changed_to, const int *h_changed_offset,
+                       const int *d_insert_heads, int n_heads, int source, const long long *h_delta,
+                       const long long *h_max_weight, const int *h_pref, long long *d_dist,
+                       int *d_parent, long long *d_comb_dist, int *d_comb_parent,
+                       mosp_sosp_stats *stats, mosp_combine_stats *cstats, void *stream) {
+  int st = checkWorkspace(ws);
+  if (st != MOSP_OK) return st;
+  if (K < 1 || K > kMaxK || h_changed_offset == nullptr || h_delta == nullptr ||
+      h_max_weight == nullptr || d_dist == nullptr || d_parent == nullptr) {
+    return fail(MOSP_ERR_INVALID, "Error: invalid MOSP update arguments.");
+  }
+  const int *outW[kMaxK], *inW[kMaxK], *chFrom[kMaxK], *chTo[kMaxK];
+  int nChanged[kMaxK];
+  long long *dist[kMaxK];
+  int *parent[kMaxK];
+  for (int k = 0; k < K; ++k) {
+    outW[k] = d_out_w + static_cast<long long>(k) * m;
+    inW[k] = d_in_w + static_cast<long long>(k) * m;
+    chFrom[k] = d_changed_from + h_changed_offset[k];
+    chTo[k] = d_changed_to + h_changed_offset[k];
+    nChanged[k] = h_changed_offset[k + 1] - h_changed_offset[k];
+    dist[k] = d_dist + static_cast<long long>(k) * n;
+    parent[k] = d_parent + static_cast<long long>(k) * n;
+  }
+  UpdateArgs a{n,     m,     K,        d_out_row, d_out_col, d_in_row, d_in_col,
+               outW,  inW,   chFrom,   chTo,      nChanged,  d_insert_heads, n_heads,
+               source, h_delta, h_max_weight, dist, parent};
+  EngineParams pu, pc;
+  int bits[kMaxK] = {0};
+  if ((st = prepareUpdate(ws, a, pu, bits)) != MOSP_OK) return st;
+  long long scale = 0;
+  int cbits = 0;
+  if ((st = prepareCombined(ws, n, K, d_parent, h_pref, source, 0, d_comb_dist, d_comb_parent, pc,
+                            scale, cbits)) != MOSP_OK) {
+    return st;
+  }
+  cudaStream_t s = asStream(stream);
+  if ((st = cleanLists(ws, s)) != MOSP_OK) return st;
+  fillLists(pu, ws, 0);
+  fillLists(pc, ws, 1);
+  if ((st = markEvent(ws, 0, s)) != MOSP_OK) return st;
+  if ((st = queueEngine(ws, pu, 0, s)) != MOSP_OK) return st;
+  if ((st = markEvent(ws, 1, s)) != MOSP_OK) return st;
+  if ((st = queueEngine(ws, pc, 1, s)) != MOSP_OK) return st;
+  if ((st = markEvent(ws, 2, s)) != MOSP_OK) return st;
+  if ((st = readControl(ws, 0, 2, s)) != MOSP_OK) return st;
+  readEvents(ws, &ws->lastUpdateMs, &ws->lastCombinedMs);
+  if ((st = controlStatus(ws, ws->hostCtl[0])) != MOSP_OK) return st;
+  if ((st = controlStatus(ws, ws->hostCtl[1])) != MOSP_OK) return st;
+  const EngineControl &cu = ws->hostCtl[0];
+  const EngineControl &cc = ws->hostCtl[1];
+  if (stats) {
+    for (int k = 0; k < K; ++k) fillStats(cu, k, bits[k], stats + k);
+  }
+  if (cstats) {
+    cstats->edges = static_cast<int>(cc.sums[0]);
+    cstats->reserved = 0;
+    cstats->scale = scale;
+    cstats->delta = mosp_default_delta(static_cast<long long>(cc.sums[0]), n,
+                                       static_cast<long long>(cc.sums[1]));
+    fillStats(cc, 0, cbits, &cstats->search);
+  }
+  return maybeResetGenerations(ws, std::max(cu.finalGen, cc.finalGen), s);
+}
+
+int mosp_path_costs(mosp_workspace *ws, int n, int m, int KG, const int *d_out_row,
+                    const int *d_out_col, const int *d_out_w, const int *d_parent, int source,
+                    long long *d_costs, void *stream) {
+  int st = checkWorkspace(ws);
+  if (st != MOSP_OK) return st;
+  if (n <= 0 || m < 0 || KG < 1 || source < 0 || source >= n || d_out_row == nullptr ||
+      d_parent == nullptr || d_costs == nullptr ||
+      (m > 0 && (d_out_col == nullptr || d_out_w == nullptr))) {
+    return fail(MOSP_ERR_INVALID, "Error: invalid path-cost arguments.");
+  }
+  if (n > ws->costN || KG > ws->costKG) {
+    const long long nn = std::max<long long>(n, ws->costN);
+    const int kk = std::max(KG, ws->costKG);
+    if ((st = deviceAlloc(&ws->edgeOf, nn)) != MOSP_OK) return st;
+    if ((st = deviceAlloc(&ws->anc0, nn)) != MOSP_OK) return st;
+    if ((st = deviceAlloc(&ws->anc1, nn)) != MOSP_OK) return st;
+    if ((st = deviceAlloc(&ws->acc0, nn * kk)) != MOSP_OK) return st;
+    if ((st = deviceAlloc(&ws->acc1, nn * kk)) != MOSP_OK) return st;
+    ws->costN = nn;
+    ws->costKG = kk;
+  }
+  cudaStream_t s = asStream(stream);
+  CostParams c{};
+  c.n = n;
+  c.m = m;
+  c.KG = KG;
+  c.source = source;
+  c.timeoutNs = ws->timeoutNs;
+  c.outRow = d_out_row;
+  c.outCol = d_out_col;
+  c.outW = d_out_w;
+  c.parent = d_parent;
+  c.edgeOf = ws->edgeOf;
+  c.anc0 = ws->anc0;
+  c.anc1 = ws->anc1;
+  c.acc0 = ws->acc0;
+  c.acc1 = ws->acc1;
+  c.costs = d_costs;
+  c.ctl = ws->ctl + 3;
+  MOSP_CUDA(cudaMemsetAsync(ws->ctl + 3, 0, sizeof(EngineControl), s));
+  MOSP_CUDA(launchCosts(c, ws->shape.costCtas, s));
+  if ((st = readControl(ws, 3, 1, s)) != MOSP_OK) return st;
+  const EngineControl &h = ws->hostCtl[3];
+  if (h.status != 0) return fail(MOSP_ERR_TIMEOUT, "Error: path-cost kernel timed out.");
+  if (h.invalid) {
+    return fail(MOSP_ERR_INVALID,
+                "Error: a tree edge (parent[v], v) of the MOSP tree is not in the graph.");
+  }
+  return MOSP_OK;
+}
+
+/// Failure-path check: runs a barrier that one CTA never reaches, with the
+/// given bound; returns the status the kernel reported (MOSP_ERR_TIMEOUT
+/// when the bounded wait works). The workspace stays usable.
+int mosp_debug_barrier_timeout(mosp_workspace *ws, long long timeout_ms, int *device_status) {
+  int st = checkWorkspace(ws);
+  if (st != MOSP_OK) return st;
+  if (timeout_ms <= 0 || timeout_ms > 10000) return fail(MOSP_ERR_INVALID, "invalid timeout");
+  cudaStream_t s = nullptr;
+  MOSP_CUDA(cudaMemsetAsync(ws->ctl + 3, 0, sizeof(EngineControl), s));
+  MOSP_CUDA(launchBarrierProbe(ws->ctl + 3, timeout_ms * 1000000LL,
+                               std::min(ws->shape.engineCtas, 8), s));
+  if ((st = readControl(ws, 3, 1, s)) != MOSP_OK) return st;
+  if (device_status) *device_status = ws->hostCtl[3].status;
+  return MOSP_OK;
+}
+
+}  // extern "C"

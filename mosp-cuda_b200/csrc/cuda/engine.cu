@@ -1,0 +1,1187 @@
+// engine.cu - persistent sm_100a kernels of the DynaMOSP update path.
+//
+// sosp_engine<Mode> runs a whole SOSP update (or an SSSP from scratch, or
+// Steps 2-3 of the MOSP update) in one cooperative launch. The phases
+// follow the reference algorithm (SMShovan/MOSP-CUDA src/sospUpdateGpu.cu:
+// 211-519 and src/combinedGraphGpu.cu:55-121), re-planned for B200:
+//
+//   * all K objectives of a MOSP update share one launch and run their
+//     phases and near-far iterations side by side, so the grid barriers
+//     (the latency floor of a high-diameter graph) are paid once for all
+//     objectives instead of K times;
+//   * one grid barrier per near-far iteration: list counters rotate
+//     through three slots and the far-pile minimum is folded into the
+//     appends, so the threshold step needs no separate reduction pass;
+//   * the barrier is a release/arrive pair on separate L2 lines with a
+//     wall-clock bound (%globaltimer): a run that stalls returns
+//     MOSP_ERR_TIMEOUT instead of hanging the GPU;
+//   * subtree invalidation packs "ancestor or flag" into one int per
+//     vertex, so a pointer-jumping step is two dependent loads;
+//   * list appends are aggregated per warp and per destination list with
+//     __match_any_sync; rows longer than a warp are expanded by the whole
+//     warp, short rows one per lane.
+//
+// Result semantics (identical to the reference): words pack
+// (distance << b | parent) and only strictly better words are kept
+// (64-bit atomicMin), so among equal distances the lowest parent id wins;
+// a vertex is expanded whenever its distance strictly decreases. The fixed
+// point does not depend on the schedule, the grid size or the bucket width.
+#include "engine.h"
+
+#include <climits>
+
+namespace mospb200 {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+// ---------------------------------------------------------------------------
+// Small device helpers
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ unsigned laneId() { return threadIdx.x & 31u; }
+
+__device__ __forceinline__ unsigned long long globalNs() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ unsigned ldAcquire(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void stRelease(unsigned *p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ int ldVolatile(const int *p) {
+  return *reinterpret_cast<const volatile int *>(p);
+}
+
+/// Word helpers for one objective.
+struct Pk {
+  int bits;
+  u64 noParent;
+  __device__ __forceinline__ u64 pack(u64 d, int p) const {
+    return bits == 0 ? d : ((d << bits) | (p < 0 ? noParent : static_cast<u64>(p)));
+  }
+  __device__ __forceinline__ u64 dist(u64 w) const { return w >> bits; }
+  __device__ __forceinline__ int parent(u64 w) const {
+    const u64 f = w & noParent;
+    return f == noParent ? -1 : static_cast<int>(f);
+  }
+};
+
+__device__ __forceinline__ Pk pkOf(const ObjectiveArgs &o) {
+  return Pk{o.parentBits, o.noParent};
+}
+
+/// Barrier bookkeeping of one CTA: the barrier epoch and the wall-clock
+/// deadline (%globaltimer) of the whole launch.
+struct Sync {
+  unsigned epoch;
+  unsigned long long deadline;
+};
+
+__device__ __forceinline__ Sync startSync(long long timeoutNs) {
+  return Sync{0u, globalNs() + static_cast<unsigned long long>(timeoutNs)};
+}
+
+/// Software grid barrier. Thread 0 of every CTA arrives on `arrive`; the
+/// last arrival publishes the epoch on `release`, which the others poll
+/// (acquire). The launch has one wall-clock deadline: a CTA that reaches a
+/// barrier after it, or waits past it, marks the run MOSP_ERR_TIMEOUT; the
+/// barrier then returns false in every CTA and the kernel must return. So a
+/// run ends by the deadline whether it stalls or keeps iterating.
+__device__ bool gridSync(EngineControl *c, Sync &sync) {
+  __shared__ int sOk;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned epoch = ++sync.epoch;
+    int ok = 1;
+    if (globalNs() > sync.deadline) atomicCAS(&c->status, 0, MOSP_ERR_TIMEOUT);
+    __threadfence();
+    const unsigned prev = atomicAdd(&c->arrive, 1u);
+    if (prev + 1u == epoch * gridDim.x) {
+      stRelease(&c->release, epoch);
+    } else {
+      unsigned spin = 0;
+      while (static_cast<int>(ldAcquire(&c->release) - epoch) < 0) {
+        if (ldVolatile(&c->status) != 0) {
+          ok = 0;
+          break;
+        }
+        if ((++spin & 127u) == 0 && globalNs() > sync.deadline) {
+          atomicCAS(&c->status, 0, MOSP_ERR_TIMEOUT);
+          ok = 0;
+          break;
+        }
+      }
+    }
+    __threadfence();
+    if (ok && ldVolatile(&c->status) != 0) ok = 0;
+    sOk = ok;
+  }
+  __syncthreads();
+  return sOk != 0;
+}
+
+/// Reserve one slot of a list: one atomicAdd per group of lanes of the warp
+/// that append to the same counter at the same time.
+__device__ __forceinline__ int warpAppend(int *counter) {
+  const unsigned mask = __activemask();
+  const unsigned peers =
+      __match_any_sync(mask, static_cast<unsigned long long>(reinterpret_cast<uintptr_t>(counter)));
+  const int leader = __ffs(peers) - 1;
+  const unsigned lane = laneId();
+  int base = 0;
+  if (static_cast<int>(lane) == leader) base = atomicAdd(counter, __popc(peers));
+  base = __shfl_sync(peers, base, leader);
+  return base + __popc(peers & ((1u << lane) - 1u));
+}
+
+/// Fold d into the minimum kept (as a complement, so 0 means "none") at
+/// *minC: one atomicMax per group of lanes with the same target.
+__device__ __forceinline__ void warpMinInto(u64 *minC, u64 d) {
+  const unsigned mask = __activemask();
+  const unsigned peers =
+      __match_any_sync(mask, static_cast<unsigned long long>(reinterpret_cast<uintptr_t>(minC)));
+  const unsigned hi = static_cast<unsigned>(d >> 32);
+  const unsigned lo = static_cast<unsigned>(d);
+  const unsigned mhi = __reduce_min_sync(peers, hi);
+  const unsigned mlo = __reduce_min_sync(peers, hi == mhi ? lo : 0xffffffffu);
+  if (static_cast<int>(laneId()) == __ffs(peers) - 1) {
+    atomicMax(minC, ~((static_cast<u64>(mhi) << 32) | mlo));
+  }
+}
+
+__device__ __forceinline__ u64 warpMinU64(u64 v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    const u64 o = __shfl_xor_sync(kFull, v, off);
+    v = o < v ? o : v;
+  }
+  return v;
+}
+
+/// Graph loads: the update and scratch modes read a graph that is
+/// read-only for the whole launch (read-only path); the combined mode
+/// reads a graph built earlier in the same launch (L2).
+template <int Mode>
+__device__ __forceinline__ int ldGraph(const int *p) {
+  if constexpr (Mode == kModeCombined) {
+    return __ldcg(p);
+  } else {
+    return __ldg(p);
+  }
+}
+
+// Shared per-CTA view of the loop state (identical in every CTA).
+struct LoopShared {
+  long long off[kMaxK + 1];
+  u64 thr[kMaxK];
+  int mode[kMaxK];
+  int fp[kMaxK];
+  int fs[kMaxK];
+  long long total;
+};
+
+enum : int { kDone = 0, kPush = 1, kSplit = 2 };
+
+// ---------------------------------------------------------------------------
+// Relaxation of one out-edge (push)
+// ---------------------------------------------------------------------------
+template <int Mode>
+__device__ __forceinline__ void relaxEdge(const EngineParams &P, const int *outCol,
+                                          const int *outW, int k, int u, u64 du,
+                                          int e, const LoopShared &L, int wrSlot,
+                                          int *nearW, int gen) {
+  const ObjectiveArgs &O = P.obj[k];
+  const int w = ldGraph<Mode>(outCol + e);
+  if (w == P.source) return;
+  const u64 nd = du + static_cast<u64>(ldGraph<Mode>(outW + e));
+  if (nd > O.maxDist) return;  // never shortest; would not fit the word
+  const Pk pk = pkOf(O);
+  const u64 cand = pk.pack(nd, u);
+  const long long base = static_cast<long long>(k) * P.stride;
+  u64 *pw = P.packed + base + w;
+  if (cand >= __ldcg(pw)) return;
+  const u64 old = atomicMin(pw, cand);
+  if (nd >= pk.dist(old)) return;  // distance did not improve
+  if (nd < L.thr[k]) {
+    if (atomicExch(P.stamp + base + w, gen) != gen) {
+      const int idx = warpAppend(&P.ctl->nearCount[k][wrSlot]);
+      nearW[base + idx] = w;
+    }
+  } else if (atomicExch(P.inFar + base + w, 1) == 0) {
+    const int fs = L.fs[k];
+    const int idx = warpAppend(&P.ctl->farCount[k][fs]);
+    (L.fp[k] == 0 ? P.farL0 : P.farL1)[base + idx] = w;
+    warpMinInto(&P.ctl->farMinC[k][fs], nd);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Near-far loop shared by every mode
+// ---------------------------------------------------------------------------
+template <int Mode>
+__device__ bool nearFarLoop(const EngineParams &P, const int *outRow,
+                            const int *outCol, const int *const *outWk,
+                            Sync &epoch, u64 *deltaOverride, int genBase) {
+  __shared__ LoopShared L;
+  EngineControl *c = P.ctl;
+  const int K = P.K;
+  const unsigned lane = laneId();
+  const int warp = threadIdx.x >> 5;
+  const long long gwarp = static_cast<long long>(blockIdx.x) * (blockDim.x >> 5) + warp;
+  const long long nwarps = static_cast<long long>(gridDim.x) * (blockDim.x >> 5);
+
+  // Per-objective loop state, held by lane k of warp 0 (same in every CTA).
+  u64 thr = 0;
+  int fp = 0, fs = 0;
+  int iters = 0, epochs = 0;
+  long long pushes = 0;
+  u64 delta = 1;
+  if (warp == 0 && static_cast<int>(lane) < K) {
+    delta = P.obj[lane].delta;
+    if (deltaOverride != nullptr && lane == 0) delta = *deltaOverride;
+  }
+
+  int it = 0;
+  for (;; ++it) {
+    const int rdSlot = it % 3, wrSlot = (it + 1) % 3, clrSlot = (it + 2) % 3;
+    if (warp == 0) {
+      const int k = static_cast<int>(lane);
+      const bool act = k < K;
+      int mode = kDone;
+      long long items = 0;
+      if (act) {
+        const int nc = __ldcg(&c->nearCount[k][rdSlot]);
+        if (nc > 0) {
+          mode = kPush;
+          items = nc;
+        } else {
+          const int fc = __ldcg(&c->farCount[k][fs]);
+          if (fc > 0) {
+            mode = kSplit;
+            items = fc;
+            const u64 mnC = __ldcg(&c->farMinC[k][fs]);
+            u64 lo = thr;
+            if (mnC != 0) {
+              const u64 mn = ~mnC;
+              lo = mn > thr ? mn : thr;
+            }
+            thr = (lo > kInfWord - delta) ? kInfWord - 1 : lo + delta;
+          }
+        }
+      }
+      // exclusive prefix of items over the objectives
+      long long incl = items;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const long long o = __shfl_up_sync(kFull, incl, off);
+        if (static_cast<int>(lane) >= off) incl += o;
+      }
+      if (act) {
+        L.off[k] = incl - items;
+        L.thr[k] = thr;
+        L.mode[k] = mode;
+        L.fp[k] = fp;
+        L.fs[k] = fs;
+      }
+      const long long total = __shfl_sync(kFull, incl, 31);
+      if (lane == 0) L.total = total;
+      if (act) {
+        if (blockIdx.x == 0) {
+          c->nearCount[k][clrSlot] = 0;
+          if (mode == kSplit) {
+            c->farCount[k][(fs + 2) % 3] = 0;
+            c->farMinC[k][(fs + 2) % 3] = 0;
+          }
+        }
+        if (mode == kPush) {
+          ++iters;
+          pushes += items;
+        } else if (mode == kSplit) {
+          ++epochs;
+          fp ^= 1;           // takes effect after this iteration
+          fs = (fs + 1) % 3;
+        }
+      }
+    }
+    __syncthreads();
+    const long long total = L.total;
+    if (total == 0) break;
+
+    const int gen = genBase + 1 + it;
+    const int *nearR = (it & 1) ? P.nearL1 : P.nearL0;
+    int *nearW = (it & 1) ? P.nearL0 : P.nearL1;
+
+    for (long long base = gwarp * 32; base < total; base += nwarps * 32) {
+      const long long j = base + lane;
+      const bool valid = j < total;
+      int k = 0;
+      if (valid) {
+        while (k + 1 < K && L.off[k + 1] <= j) ++k;
+      }
+      const int mode = valid ? L.mode[k] : kDone;
+      const long long i = valid ? j - L.off[k] : 0;
+      const long long ko = static_cast<long long>(k) * P.stride;
+
+      if (mode == kSplit) {
+        // far pile entry: back to the near list below the new threshold
+        const int v = __ldcg((L.fp[k] == 0 ? P.farL0 : P.farL1) + ko + i);
+        const u64 word = __ldcg(P.packed + ko + v);
+        const Pk pk = pkOf(P.obj[k]);
+        const u64 d = word == kInfWord ? kInfWord : pk.dist(word);
+        if (d < L.thr[k]) {
+          P.inFar[ko + v] = 0;
+          if (atomicExch(P.stamp + ko + v, gen) != gen) {
+            const int idx = warpAppend(&c->nearCount[k][wrSlot]);
+            nearW[ko + idx] = v;
+          }
+        } else {
+          const int nfs = (L.fs[k] + 1) % 3;
+          const int idx = warpAppend(&c->farCount[k][nfs]);
+          (L.fp[k] == 0 ? P.farL1 : P.farL0)[ko + idx] = v;
+          warpMinInto(&c->farMinC[k][nfs], d);
+        }
+      }
+
+      // push: expand the near-list vertex of this lane
+      int u = -1, beg = 0, end = 0;
+      u64 du = 0;
+      if (mode == kPush) {
+        u = __ldcg(nearR + ko + i);
+        const u64 word = __ldcg(P.packed + ko + u);
+        if (word != kInfWord) {
+          du = pkOf(P.obj[k]).dist(word);
+          beg = ldGraph<Mode>(outRow + u);
+          end = ldGraph<Mode>(outRow + u + 1);
+        }
+      }
+      const int deg = end - beg;
+      unsigned big = __ballot_sync(kFull, deg > kLaneRowMax);
+      if (deg > 0 && deg <= kLaneRowMax) {
+        const int *w = outWk[k];
+        for (int e = beg; e < end; ++e) {
+          relaxEdge<Mode>(P, outCol, w, k, u, du, e, L, wrSlot, nearW, gen);
+        }
+      }
+      while (big != 0) {
+        const int src = __ffs(big) - 1;
+        big &= big - 1;
+        const int kb = __shfl_sync(kFull, k, src);
+        const int ub = __shfl_sync(kFull, u, src);
+        const u64 db = __shfl_sync(kFull, du, src);
+        const int bb = __shfl_sync(kFull, beg, src);
+        const int eb = __shfl_sync(kFull, end, src);
+        const int *w = outWk[kb];
+        for (int e = bb + static_cast<int>(lane); e < eb; e += 32) {
+          relaxEdge<Mode>(P, outCol, w, kb, ub, db, e, L, wrSlot, nearW, gen);
+        }
+      }
+    }
+    if (!gridSync(c, epoch)) return false;
+  }
+
+  if (blockIdx.x == 0 && warp == 0 && static_cast<int>(lane) < K) {
+    c->iterations[lane] = iters;
+    c->epochs[lane] = epochs;
+    c->pushes[lane] = pushes;
+    if (lane == 0) {
+      c->finalGen = genBase + 1 + it;
+      *P.genPtr = genBase + 1 + it;
+    }
+  }
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// Unpack words into (distance, parent); distance-only objectives recover
+// the lowest-id tight parent (reference src/sospUpdateGpu.cu:478-512).
+// ---------------------------------------------------------------------------
+template <int Mode>
+__device__ bool unpackResults(const EngineParams &P, const int *outRow,
+                              const int *outCol, const int *const *outWk,
+                              Sync &epoch) {
+  const int n = P.n, K = P.K;
+  const long long tid = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const long long T = static_cast<long long>(gridDim.x) * blockDim.x;
+  bool anyFallback = false;
+  for (int k = 0; k < K; ++k) {
+    const ObjectiveArgs &O = P.obj[k];
+    const Pk pk = pkOf(O);
+    const long long ko = static_cast<long long>(k) * P.stride;
+    if (O.parentBits > 0) {
+      for (long long v = tid; v < n; v += T) {
+        const u64 word = __ldcg(P.packed + ko + v);
+        if (word == kInfWord) {
+          O.dist[v] = kDistInf;
+          O.parent[v] = -1;
+        } else {
+          O.dist[v] = static_cast<long long>(pk.dist(word));
+          O.parent[v] = pk.parent(word);
+        }
+      }
+    } else {
+      anyFallback = true;
+      for (long long v = tid; v < n; v += T) {
+        const u64 word = __ldcg(P.packed + ko + v);
+        O.dist[v] = word == kInfWord ? kDistInf : static_cast<long long>(word);
+        O.parent[v] = (word == kInfWord || v == P.source) ? -1 : INT_MAX;
+      }
+    }
+  }
+  if (!anyFallback) return true;
+  if (!gridSync(P.ctl, epoch)) return false;
+  const unsigned lane = laneId();
+  const long long gwarp = tid >> 5;
+  const long long nwarps = T >> 5;
+  for (int k = 0; k < K; ++k) {
+    const ObjectiveArgs &O = P.obj[k];
+    if (O.parentBits > 0) continue;
+    const long long ko = static_cast<long long>(k) * P.stride;
+    const int *w = outWk[k];
+    for (long long base = gwarp * 32; base < n; base += nwarps * 32) {
+      const long long uu = base + lane;
+      int beg = 0, end = 0;
+      u64 du = kInfWord;
+      if (uu < n) {
+        du = __ldcg(P.packed + ko + uu);
+        if (du != kInfWord) {
+          beg = ldGraph<Mode>(outRow + uu);
+          end = ldGraph<Mode>(outRow + uu + 1);
+        }
+      }
+      const int deg = end - beg;
+      unsigned big = __ballot_sync(kFull, deg > kLaneRowMax);
+      if (deg > 0 && deg <= kLaneRowMax) {
+        for (int e = beg; e < end; ++e) {
+          const int x = ldGraph<Mode>(outCol + e);
+          if (x != P.source &&
+              du + static_cast<u64>(ldGraph<Mode>(w + e)) == __ldcg(P.packed + ko + x)) {
+            atomicMin(O.parent + x, static_cast<int>(uu));
+          }
+        }
+      }
+      while (big != 0) {
+        const int src = __ffs(big) - 1;
+        big &= big - 1;
+        const int ub = static_cast<int>(__shfl_sync(kFull, uu, src));
+        const u64 db = __shfl_sync(kFull, du, src);
+        const int bb = __shfl_sync(kFull, beg, src);
+        const int eb = __shfl_sync(kFull, end, src);
+        for (int e = bb + static_cast<int>(lane); e < eb; e += 32) {
+          const int x = ldGraph<Mode>(outCol + e);
+          if (x != P.source &&
+              db + static_cast<u64>(ldGraph<Mode>(w + e)) == __ldcg(P.packed + ko + x)) {
+            atomicMin(O.parent + x, ub);
+          }
+        }
+      }
+    }
+  }
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// Block-level scan helpers (combined-graph and reverse-CSR builds)
+// ---------------------------------------------------------------------------
+
+/// Inclusive scan of one value per thread over the CTA; *total = CTA sum.
+__device__ long long blockInclusiveScan(long long x, long long *total) {
+  __shared__ long long warpSums[kThreads / 32];
+  const unsigned lane = laneId();
+  const int warp = threadIdx.x >> 5;
+  long long v = x;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const long long o = __shfl_up_sync(kFull, v, off);
+    if (static_cast<int>(lane) >= off) v += o;
+  }
+  if (lane == 31) warpSums[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = blockDim.x >> 5;
+    long long s = static_cast<int>(lane) < nw ? warpSums[lane] : 0;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const long long o = __shfl_up_sync(kFull, s, off);
+      if (static_cast<int>(lane) >= off) s += o;
+    }
+    if (static_cast<int>(lane) < nw) warpSums[lane] = s;
+  }
+  __syncthreads();
+  const long long prefix = warp > 0 ? warpSums[warp - 1] : 0;
+  *total = warpSums[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return prefix + v;
+}
+
+/// Sum of one value per thread over the CTA (every thread gets it).
+__device__ long long blockSum(long long x) {
+  long long total;
+  blockInclusiveScan(x, &total);
+  return total;
+}
+
+/// Exclusive scan in[0, len) -> out[0, len) (and copy -> cursor) across the
+/// grid; two phases separated by one grid barrier. Returns the total.
+__device__ bool gridExclusiveScan(const int *in, int *out, int *cursor, long long len,
+                                  long long *blockSums, EngineControl *c,
+                                  Sync &epoch, long long *grandTotal) {
+  const long long chunk = (len + gridDim.x - 1) / gridDim.x;
+  const long long lo = static_cast<long long>(blockIdx.x) * chunk;
+  const long long hi = lo + chunk < len ? lo + chunk : len;
+  long long local = 0;
+  for (long long i = lo + threadIdx.x; i < hi; i += blockDim.x) local += __ldcg(in + i);
+  const long long sum = blockSum(local);
+  if (threadIdx.x == 0) blockSums[blockIdx.x] = sum;
+  if (!gridSync(c, epoch)) return false;
+  long long before = 0, all = 0;
+  for (int b = threadIdx.x; b < static_cast<int>(gridDim.x); b += blockDim.x) {
+    const long long s = __ldcg(blockSums + b);
+    all += s;
+    if (b < static_cast<int>(blockIdx.x)) before += s;
+  }
+  before = blockSum(before);
+  all = blockSum(all);
+  long long carry = before;
+  for (long long t = lo; t < hi; t += blockDim.x) {
+    const long long i = t + threadIdx.x;
+    const long long x = i < hi ? __ldcg(in + i) : 0;
+    long long tileTotal;
+    const long long incl = blockInclusiveScan(x, &tileTotal);
+    if (i < hi) {
+      out[i] = static_cast<int>(carry + incl - x);
+      if (cursor != nullptr) cursor[i] = static_cast<int>(carry + incl - x);
+    }
+    carry += tileTotal;
+  }
+  *grandTotal = all;
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// Combined graph edge of parent k of v (reference
+// src/combinedGraphGpu.cu:55-75): edge (p, v) is attributed to the first
+// tree whose parent of v is p; its weight is base - sum of the preference
+// terms of every tree with that parent.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool combinedEdge(const EngineParams &P, int v, int k,
+                                             int &p, int &weight) {
+  const long long n = P.n;
+  p = __ldg(P.combParents + k * n + v);
+  if (p < 0) return false;
+  for (int j = 0; j < k; ++j) {
+    if (__ldg(P.combParents + j * n + v) == p) return false;
+  }
+  weight = P.combBase - P.prefTerms[k];
+  for (int j = k + 1; j < P.combK; ++j) {
+    if (__ldg(P.combParents + j * n + v) == p) weight -= P.prefTerms[j];
+  }
+  return true;
+}
+
+template <int Mode>
+__device__ void scratchOrCombined(const EngineParams &P, Sync &epoch, int genBase,
+                                  const int **sOutWk);
+
+// ---------------------------------------------------------------------------
+// The engine kernel
+// ---------------------------------------------------------------------------
+template <int Mode>
+__global__ void __launch_bounds__(kThreads, 1) sospEngine(const __grid_constant__ EngineParams P) {
+  EngineControl *c = P.ctl;
+  const int n = P.n, K = P.K;
+  const long long tid = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const long long T = static_cast<long long>(gridDim.x) * blockDim.x;
+  const unsigned lane = laneId();
+  const int warp = threadIdx.x >> 5;
+  const long long gwarp = tid >> 5;
+  const long long nwarps = T >> 5;
+  Sync epoch = startSync(P.timeoutNs);
+  // Stamp generations of this launch start after the previous launch's.
+  const int genBase = __ldcg(P.genPtr) + 1;
+
+  __shared__ const int *sOutWk[kMaxK];
+  if (threadIdx.x < kMaxK) {
+    sOutWk[threadIdx.x] =
+        static_cast<int>(threadIdx.x) < K ? P.obj[threadIdx.x].outW : nullptr;
+  }
+  const int *outRow = P.outRow;
+  const int *outCol = P.outCol;
+
+  if constexpr (Mode == kModeUpdate) {
+    // ---- Pack the old trees; ancestors (reference :234-252) ---------------
+    for (int k = 0; k < K; ++k) {
+      const ObjectiveArgs &O = P.obj[k];
+      const Pk pk = pkOf(O);
+      const long long ko = static_cast<long long>(k) * P.stride;
+      for (long long v = tid; v < n; v += T) {
+        const long long d = O.dist[v];
+        int p = O.parent[v];
+        if (p < -1 || p >= n) {
+          c->invalid = 1;
+          p = -1;
+        }
+        u64 word;
+        if (d >= kDistInf / 2) {
+          word = kInfWord;
+        } else if (d < 0 || static_cast<u64>(d) > O.maxDist) {
+          c->overflow = 1;
+          word = kInfWord;
+        } else {
+          word = pk.pack(static_cast<u64>(d), p);
+        }
+        P.packed[ko + v] = word;
+        P.val[ko + v] = p;  // >= 0: ancestor; -1: none; -2: invalidated
+      }
+    }
+    if (!gridSync(c, epoch)) return;
+
+    // ---- Roots: heads of changed tree edges -------------------------------
+    long long changes = 0;
+    for (int k = 0; k < K; ++k) {
+      const ObjectiveArgs &O = P.obj[k];
+      const long long ko = static_cast<long long>(k) * P.stride;
+      changes += O.nChanged;
+      for (long long i = tid; i < O.nChanged; i += T) {
+        const int v = O.chTo[i], u = O.chFrom[i];
+        if (v < 0 || v >= n || u < 0 || u >= n) {
+          c->invalid = 1;
+          continue;
+        }
+        if (O.parent[v] == u) P.val[ko + v] = -2;
+      }
+    }
+    if (!gridSync(c, epoch)) return;
+
+    // ---- Subtree invalidation by pointer jumping (reference :254-291) -----
+    // val[v] >= 0: no root on the tree path from v up to (excluding)
+    // val[v]; -1: no root above v at all; -2: a root is v or an ancestor.
+    // Every value another thread can observe keeps this invariant, so the
+    // updates are made in place.
+    if (changes > 0) {
+      for (int round = 0; round < P.maxRounds; ++round) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+          c->jumpActive[(round + 1) % 3] = 0;
+          c->rounds = round + 1;
+        }
+        int jumping = 0;
+        for (int k = 0; k < K; ++k) {
+          if (P.obj[k].nChanged == 0) continue;
+          int *val = P.val + static_cast<long long>(k) * P.stride;
+          for (long long v = tid; v < n; v += T) {
+            const int a = __ldcg(val + v);
+            if (a < 0) continue;
+            const int b = __ldcg(val + a);
+            if (b == -2 || b == -1) {
+              val[v] = b;
+            } else {
+              val[v] = b;
+              jumping = 1;
+            }
+          }
+        }
+        if (__syncthreads_or(jumping) && threadIdx.x == 0) {
+          atomicOr(&c->jumpActive[round % 3], 1);
+        }
+        if (!gridSync(c, epoch)) return;
+        if (__ldcg(&c->jumpActive[round % 3]) == 0) break;
+        if (round + 1 == P.maxRounds && blockIdx.x == 0 && threadIdx.x == 0) {
+          c->invalid = 1;  // the parent arrays are not a forest
+        }
+      }
+    }
+
+    // ---- Invalidate; candidates = invalidated + insert heads (:293-313) ---
+    for (int k = 0; k < K; ++k) {
+      const long long ko = static_cast<long long>(k) * P.stride;
+      for (long long base = gwarp * 32; base < n; base += nwarps * 32) {
+        const long long v = base + lane;
+        const bool inv = v < n && __ldcg(P.val + ko + v) == -2;
+        const unsigned ballot = __ballot_sync(kFull, inv);
+        if (inv) {
+          P.packed[ko + v] = kInfWord;
+          const int idx = warpAppend(&c->candCount[k]);
+          P.cand[ko + idx] = static_cast<int>(v);
+        }
+        if (lane == 0 && ballot != 0) atomicAdd(&c->invalidated[k], __popc(ballot));
+      }
+      for (long long i = tid; i < P.nHeads; i += T) {
+        const int v = P.heads[i];
+        if (v < 0 || v >= n) {
+          c->invalid = 1;
+          continue;
+        }
+        if (v == P.source || __ldcg(P.val + ko + v) == -2) continue;
+        if (atomicExch(P.stamp + ko + v, genBase) != genBase) {
+          const int idx = warpAppend(&c->candCount[k]);
+          P.cand[ko + idx] = v;
+        }
+      }
+    }
+    if (!gridSync(c, epoch)) return;
+
+    // ---- Pull pass over in-edges (reference :315-344) ----------------------
+    // The improved candidates form far pile 0; the first iteration of the
+    // loop sets the threshold to their minimum + delta and splits them.
+    {
+      __shared__ long long sOff[kMaxK + 1];
+      if (warp == 0) {
+        const long long cnt =
+            static_cast<int>(lane) < K ? __ldcg(&c->candCount[lane]) : 0;
+        long long incl = cnt;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+          const long long o = __shfl_up_sync(kFull, incl, off);
+          if (static_cast<int>(lane) >= off) incl += o;
+        }
+        sOff[lane] = incl - cnt;
+        if (lane == 31) sOff[kMaxK] = incl;
+      }
+      __syncthreads();
+      const long long total = sOff[kMaxK];
+      for (long long base = gwarp * 32; base < total; base += nwarps * 32) {
+        const long long j = base + lane;
+        const bool valid = j < total;
+        int k = 0;
+        if (valid) {
+          while (k + 1 < K && sOff[k + 1] <= j) ++k;
+        }
+        const long long ko = static_cast<long long>(k) * P.stride;
+        const ObjectiveArgs &O = P.obj[k];
+        const Pk pk = pkOf(O);
+        int v = -1, beg = 0, end = 0;
+        u64 cur = kInfWord;
+        if (valid) {
+          v = __ldcg(P.cand + ko + (j - sOff[k]));
+          cur = __ldcg(P.packed + ko + v);
+          beg = __ldg(P.inRow + v);
+          end = __ldg(P.inRow + v + 1);
+        }
+        u64 best = cur;
+        const int deg = end - beg;
+        unsigned big = __ballot_sync(kFull, deg > kLaneRowMax);
+        if (deg <= kLaneRowMax) {
+          for (int e = beg; e < end; ++e) {
+            const int u = __ldg(P.inCol + e);
+            const u64 wd = __ldcg(P.packed + ko + u);
+            if (wd == kInfWord) continue;
+            const u64 nd = pk.dist(wd) + static_cast<u64>(__ldg(O.inW + e));
+            if (nd <= O.maxDist) {
+              const u64 cw = pk.pack(nd, u);
+              best = cw < best ? cw : best;
+            }
+          }
+        }
+        while (big != 0) {
+          const int src = __ffs(big) - 1;
+          big &= big - 1;
+          const int kb = __shfl_sync(kFull, k, src);
+          const int bb = __shfl_sync(kFull, beg, src);
+          const int eb = __shfl_sync(kFull, end, src);
+          const ObjectiveArgs &Ob = P.obj[kb];
+          const Pk pb = pkOf(Ob);
+          const long long kob = static_cast<long long>(kb) * P.stride;
+          u64 part = kInfWord;
+          for (int e = bb + static_cast<int>(lane); e < eb; e += 32) {
+            const int u = __ldg(P.inCol + e);
+            const u64 wd = __ldcg(P.packed + kob + u);
+            if (wd == kInfWord) continue;
+            const u64 nd = pb.dist(wd) + static_cast<u64>(__ldg(Ob.inW + e));
+            if (nd <= Ob.maxDist) {
+              const u64 cw = pb.pack(nd, u);
+              part = cw < part ? cw : part;
+            }
+          }
+          part = warpMinU64(part);
+          if (static_cast<int>(lane) == src) best = part < best ? part : best;
+        }
+        if (valid && best < cur) {
+          // only this thread writes the word of v during the pull pass
+          P.packed[ko + v] = best;
+          if (pk.dist(best) < (cur == kInfWord ? kInfWord : pk.dist(cur))) {
+            P.inFar[ko + v] = 1;
+            const int idx = warpAppend(&c->farCount[k][0]);
+            P.farL0[ko + idx] = v;
+            warpMinInto(&c->farMinC[k][0], pk.dist(best));
+          }
+        }
+      }
+    }
+    if (!gridSync(c, epoch)) return;
+    if (!nearFarLoop<Mode>(P, outRow, outCol, sOutWk, epoch, nullptr, genBase)) return;
+    unpackResults<Mode>(P, outRow, outCol, sOutWk, epoch);
+  } else {
+    scratchOrCombined<Mode>(P, epoch, genBase, sOutWk);
+  }
+}
+
+/// Steps 2-3 (combined mode) and the SSSP from scratch (both modes).
+template <int Mode>
+__device__ void scratchOrCombined(const EngineParams &P, Sync &epoch, int genBase,
+                                  const int **sOutWk) {
+  EngineControl *c = P.ctl;
+  const int n = P.n, K = P.K;
+  const long long tid = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const long long T = static_cast<long long>(gridDim.x) * blockDim.x;
+  const unsigned lane = laneId();
+  __shared__ u64 sCombDelta;
+  const int *outRow = P.outRow;
+  const int *outCol = P.outCol;
+
+  if constexpr (Mode == kModeCombined) {
+    // ---- Step 2: combined graph, count / scan / fill (reference
+    // src/combinedGraphGpu.cu:80-121, 281-300), then Step 3 below --------
+    for (long long v = tid; v <= n; v += T) P.combDeg[v] = 0;
+    if (!gridSync(c, epoch)) return;
+    unsigned long long edges = 0, wsum = 0;
+    for (long long v = tid; v < n; v += T) {
+      if (v == P.source) continue;
+      for (int k = 0; k < P.combK; ++k) {
+        int p, w;
+        if (combinedEdge(P, static_cast<int>(v), k, p, w)) {
+          if (p >= n) {
+            c->invalid = 1;
+            continue;
+          }
+          atomicAdd(P.combDeg + p, 1);
+          ++edges;
+          wsum += static_cast<unsigned long long>(w);
+        }
+      }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      edges += __shfl_down_sync(kFull, edges, off);
+      wsum += __shfl_down_sync(kFull, wsum, off);
+    }
+    if (lane == 0 && edges > 0) {
+      atomicAdd(&c->sums[0], edges);
+      atomicAdd(&c->sums[1], wsum);
+    }
+    if (!gridSync(c, epoch)) return;
+    long long totalEdges = 0;
+    if (__ldcg(&c->invalid) != 0) return;
+    // row starts; the degree array becomes the fill cursor (each CTA reads
+    // and rewrites only its own chunk)
+    if (!gridExclusiveScan(P.combDeg, P.combRow, P.combDeg, static_cast<long long>(n) + 1,
+                           P.blockSums, c, epoch, &totalEdges)) {
+      return;
+    }
+    if (!gridSync(c, epoch)) return;
+    for (long long v = tid; v < n; v += T) {
+      if (v == P.source) continue;
+      for (int k = 0; k < P.combK; ++k) {
+        int p, w;
+        if (combinedEdge(P, static_cast<int>(v), k, p, w)) {
+          const int pos = atomicAdd(P.combDeg + p, 1);
+          P.combCol[pos] = static_cast<int>(v);
+          P.combW[pos] = w;
+        }
+      }
+    }
+    if (threadIdx.x == 0) {
+      // Default bucket width of the combined graph (reference
+      // src/combinedGraphGpu.cu:310-312 and :607-616 of sospUpdateGpu.cu).
+      u64 d = static_cast<u64>(P.combDelta);
+      if (P.combDelta <= 0) {
+        const double e = static_cast<double>(__ldcg(&c->sums[0]));
+        const double ws = static_cast<double>(__ldcg(&c->sums[1]));
+        long long dd = 1;
+        if (e > 0 && n > 0) {
+          dd = static_cast<long long>(32.0 * (ws / e) / (e / static_cast<double>(n)));
+          if (dd < 1) dd = 1;
+        }
+        d = static_cast<u64>(dd);
+      }
+      sCombDelta = d;
+    }
+    outRow = P.combRow;
+    outCol = P.combCol;
+    if (threadIdx.x == 0) sOutWk[0] = P.combW;
+    // fall through to the SSSP from scratch
+  }
+
+  // ---- SSSP from scratch: only the source is finite ------------------------
+  for (int k = 0; k < K; ++k) {
+    const Pk pk = pkOf(P.obj[k]);
+    const long long ko = static_cast<long long>(k) * P.stride;
+    for (long long v = tid; v < n; v += T) {
+      P.packed[ko + v] = v == P.source ? pk.pack(0, -1) : kInfWord;
+    }
+    if (tid == 0) {
+      P.inFar[ko + P.source] = 1;
+      P.farL0[ko] = P.source;
+      c->farCount[k][0] = 1;
+      c->farMinC[k][0] = ~0ULL;  // minimum 0
+    }
+  }
+  if (!gridSync(c, epoch)) return;
+  u64 *deltaOverride = nullptr;
+  if constexpr (Mode == kModeCombined) deltaOverride = &sCombDelta;
+  if (!nearFarLoop<Mode>(P, outRow, outCol, sOutWk, epoch, deltaOverride, genBase)) return;
+  unpackResults<Mode>(P, outRow, outCol, sOutWk, epoch);
+}
+
+// ---------------------------------------------------------------------------
+// Device graph: objective-major weights and the reverse CSR (reference
+// src/deviceGraph.cu:28-63, 87-135), one cooperative launch.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads, 1) buildGraph(const __grid_constant__ BuildParams B) {
+  EngineControl *c = B.ctl;
+  const int n = B.n, m = B.m, K = B.K;
+  const long long tid = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const long long T = static_cast<long long>(gridDim.x) * blockDim.x;
+  const unsigned lane = laneId();
+  const long long gwarp = tid >> 5, nwarps = T >> 5;
+  Sync epoch = startSync(B.timeoutNs);
+
+  // validate the CSR; split the weights; clear the degree counts
+  if (tid == 0 && (__ldg(B.outRow) != 0 || __ldg(B.outRow + n) != m)) c->invalid = 1;
+  for (long long v = tid; v < n; v += T) {
+    if (__ldg(B.outRow + v + 1) < __ldg(B.outRow + v)) c->invalid = 1;
+  }
+  for (long long e = tid; e < m; e += T) {
+    const int x = __ldg(B.outCol + e);
+    if (x < 0 || x >= n) c->invalid = 1;
+  }
+  for (long long i = tid; i < static_cast<long long>(m) * K; i += T) {
+    const long long e = i / K;
+    const int k = static_cast<int>(i - e * K);
+    B.outW[static_cast<long long>(k) * m + e] = __ldg(B.edgeMajorW + i);
+  }
+  for (long long v = tid; v <= n; v += T) B.cursor[v] = 0;
+  if (!gridSync(c, epoch)) return;
+  if (__ldcg(&c->invalid) != 0) return;
+
+  for (long long e = tid; e < m; e += T) atomicAdd(B.cursor + __ldg(B.outCol + e), 1);
+  if (!gridSync(c, epoch)) return;
+  long long total = 0;
+  if (!gridExclusiveScan(B.cursor, B.inRow, B.cursor, static_cast<long long>(n) + 1,
+                         B.blockSums, c, epoch, &total)) {
+    return;
+  }
+  if (!gridSync(c, epoch)) return;
+
+  // fill: one lane per short row, one warp per long row
+  for (long long base = gwarp * 32; base < n; base += nwarps * 32) {
+    const long long u = base + lane;
+    int beg = 0, end = 0;
+    if (u < n) {
+      beg = __ldg(B.outRow + u);
+      end = __ldg(B.outRow + u + 1);
+    }
+    const int deg = end - beg;
+    unsigned big = __ballot_sync(kFull, deg > kLaneRowMax);
+    auto place = [&](int uu, int e) {
+      const int pos = atomicAdd(B.cursor + __ldg(B.outCol + e), 1);
+      B.inCol[pos] = uu;
+      for (int k = 0; k < K; ++k) {
+        B.inW[static_cast<long long>(k) * m + pos] =
+            __ldg(B.edgeMajorW + static_cast<long long>(e) * K + k);
+      }
+    };
+    if (deg <= kLaneRowMax) {
+      for (int e = beg; e < end; ++e) place(static_cast<int>(u), e);
+    }
+    while (big != 0) {
+      const int src = __ffs(big) - 1;
+      big &= big - 1;
+      const int ub = static_cast<int>(__shfl_sync(kFull, u, src));
+      const int bb = __shfl_sync(kFull, beg, src);
+      const int eb = __shfl_sync(kFull, end, src);
+      for (int e = bb + static_cast<int>(lane); e < eb; e += 32) place(ub, e);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// MOSP path costs: sums of the original weights along the MOSP tree by
+// pointer jumping with double buffering (replaces the host BFS of
+// reference src/combinedGraphGpu.cu:161-208; same edge rule: the first
+// occurrence of v in row p).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ long long satAdd(long long a, long long b) {
+  if (a >= kDistInf / 2 || b >= kDistInf / 2) return kDistInf;
+  const long long s = a + b;
+  return s >= kDistInf / 2 ? kDistInf : s;
+}
+
+__global__ void __launch_bounds__(kThreads, 1) pathCosts(const __grid_constant__ CostParams C) {
+  EngineControl *c = C.ctl;
+  const int n = C.n, KG = C.KG;
+  const long long tid = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const long long T = static_cast<long long>(gridDim.x) * blockDim.x;
+  const unsigned lane = laneId();
+  const long long gwarp = tid >> 5, nwarps = T >> 5;
+  Sync epoch = startSync(C.timeoutNs);
+
+  for (long long v = tid; v < n; v += T) C.edgeOf[v] = INT_MAX;
+  if (!gridSync(c, epoch)) return;
+  // first occurrence of the tree edge (parent[v], v): lowest e in row p
+  for (long long base = gwarp * 32; base < n; base += nwarps * 32) {
+    const long long u = base + lane;
+    int beg = 0, end = 0;
+    if (u < n) {
+      beg = __ldg(C.outRow + u);
+      end = __ldg(C.outRow + u + 1);
+    }
+    const int deg = end - beg;
+    unsigned big = __ballot_sync(kFull, deg > kLaneRowMax);
+    if (deg <= kLaneRowMax) {
+      for (int e = beg; e < end; ++e) {
+        const int v = __ldg(C.outCol + e);
+        if (v != C.source && __ldg(C.parent + v) == u) atomicMin(C.edgeOf + v, e);
+      }
+    }
+    while (big != 0) {
+      const int src = __ffs(big) - 1;
+      big &= big - 1;
+      const int ub = static_cast<int>(__shfl_sync(kFull, u, src));
+      const int bb = __shfl_sync(kFull, beg, src);
+      const int eb = __shfl_sync(kFull, end, src);
+      for (int e = bb + static_cast<int>(lane); e < eb; e += 32) {
+        const int v = __ldg(C.outCol + e);
+        if (v != C.source && __ldg(C.parent + v) == ub) atomicMin(C.edgeOf + v, e);
+      }
+    }
+  }
+  if (!gridSync(c, epoch)) return;
+  for (long long v = tid; v < n; v += T) {
+    const int p = __ldg(C.parent + v);
+    long long *acc = C.acc0 + v * KG;
+    if (v == C.source) {
+      C.anc0[v] = -1;
+      for (int k = 0; k < KG; ++k) acc[k] = 0;
+    } else if (p < 0 || p >= n) {
+      if (p >= n) c->invalid = 1;
+      C.anc0[v] = -1;
+      for (int k = 0; k < KG; ++k) acc[k] = kDistInf;
+    } else {
+      const int e = __ldcg(C.edgeOf + v);
+      if (e == INT_MAX) {
+        c->invalid = 1;  // the tree edge is not in the graph
+        C.anc0[v] = -1;
+        for (int k = 0; k < KG; ++k) acc[k] = kDistInf;
+      } else {
+        C.anc0[v] = p;
+        for (int k = 0; k < KG; ++k) {
+          acc[k] = __ldg(C.outW + static_cast<long long>(k) * C.m + e);
+        }
+      }
+    }
+  }
+  if (!gridSync(c, epoch)) return;
+  int round = 0;
+  for (;; ++round) {
+    const int *ancR = (round & 1) ? C.anc1 : C.anc0;
+    int *ancW = (round & 1) ? C.anc0 : C.anc1;
+    const long long *accR = (round & 1) ? C.acc1 : C.acc0;
+    long long *accW = (round & 1) ? C.acc0 : C.acc1;
+    if (blockIdx.x == 0 && threadIdx.x == 0) c->jumpActive[(round + 1) % 3] = 0;
+    int active = 0;
+    for (long long v = tid; v < n; v += T) {
+      const int a = __ldcg(ancR + v);
+      if (a >= 0) {
+        const int b = __ldcg(ancR + a);
+        for (int k = 0; k < KG; ++k) {
+          accW[v * KG + k] = satAdd(__ldcg(accR + v * KG + k), __ldcg(accR + static_cast<long long>(a) * KG + k));
+        }
+        ancW[v] = b;
+        active |= b >= 0;
+      } else {
+        for (int k = 0; k < KG; ++k) accW[v * KG + k] = __ldcg(accR + v * KG + k);
+        ancW[v] = a;
+      }
+    }
+    if (__syncthreads_or(active) && threadIdx.x == 0) atomicOr(&c->jumpActive[round % 3], 1);
+    if (!gridSync(c, epoch)) return;
+    if (__ldcg(&c->jumpActive[round % 3]) == 0 || round > 64) break;
+  }
+  const long long *accF = (round & 1) ? C.acc0 : C.acc1;
+  for (long long i = tid; i < static_cast<long long>(n) * KG; i += T) {
+    const long long x = __ldcg(accF + i);
+    C.costs[i] = x >= kDistInf / 2 ? kDistInf : x;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Failure-path probe: every CTA but the first waits at a barrier that the
+// first never reaches; the bounded wait must end with MOSP_ERR_TIMEOUT.
+// ---------------------------------------------------------------------------
+__global__ void barrierProbe(EngineControl *c, long long timeoutNs) {
+  Sync epoch = startSync(timeoutNs);
+  if (blockIdx.x == 0) return;
+  gridSync(c, epoch);
+}
+
+template <typename Kernel>
+cudaError_t ctasFor(Kernel kernel, int sms, int ctasPerSm, int &ctas) {
+  int perSm = 0;
+  cudaError_t err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, kThreads, 0);
+  if (err != cudaSuccess) return err;
+  if (perSm < 1) return cudaErrorInvalidConfiguration;
+  if (ctasPerSm > 0 && ctasPerSm < perSm) perSm = ctasPerSm;
+  ctas = perSm * sms;
+  return cudaSuccess;
+}
+
+}  // namespace
+
+cudaError_t queryLaunchShape(int ctasPerSm, LaunchShape &shape) {
+  int device = 0, sms = 0, coop = 0;
+  cudaError_t err = cudaGetDevice(&device);
+  if (err == cudaSuccess) err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (err == cudaSuccess) err = cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
+  if (err != cudaSuccess) return err;
+  if (!coop) return cudaErrorNotSupported;
+  int a = 0, b = 0, d = 0, e = 0;
+  if ((err = ctasFor(sospEngine<kModeUpdate>, sms, ctasPerSm, a)) != cudaSuccess) return err;
+  if ((err = ctasFor(sospEngine<kModeScratch>, sms, ctasPerSm, b)) != cudaSuccess) return err;
+  if ((err = ctasFor(sospEngine<kModeCombined>, sms, ctasPerSm, d)) != cudaSuccess) return err;
+  shape.engineCtas = a < b ? (a < d ? a : d) : (b < d ? b : d);
+  if ((err = ctasFor(buildGraph, sms, ctasPerSm, e)) != cudaSuccess) return err;
+  shape.buildCtas = e;
+  if ((err = ctasFor(pathCosts, sms, ctasPerSm, e)) != cudaSuccess) return err;
+  shape.costCtas = e;
+  return cudaSuccess;
+}
+
+cudaError_t launchEngine(const EngineParams &p, int ctas, cudaStream_t s) {
+  void *args[] = {const_cast<EngineParams *>(&p)};
+  const void *fn = nullptr;
+  switch (p.mode) {
+    case kModeUpdate: fn = reinterpret_cast<const void *>(sospEngine<kModeUpdate>); break;
+    case kModeScratch: fn = reinterpret_cast<const void *>(sospEngine<kModeScratch>); break;
+    default: fn = reinterpret_cast<const void *>(sospEngine<kModeCombined>); break;
+  }
+  return cudaLaunchCooperativeKernel(fn, dim3(ctas), dim3(kThreads), args, 0, s);
+}
+
+cudaError_t launchBuild(const BuildParams &p, int ctas, cudaStream_t s) {
+  void *args[] = {const_cast<BuildParams *>(&p)};
+  return cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(buildGraph), dim3(ctas),
+                                     dim3(kThreads), args, 0, s);
+}
+
+cudaError_t launchCosts(const CostParams &p, int ctas, cudaStream_t s) {
+  void *args[] = {const_cast<CostParams *>(&p)};
+  return cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(pathCosts), dim3(ctas),
+                                     dim3(kThreads), args, 0, s);
+}
+
+cudaError_t launchBarrierProbe(EngineControl *ctl, long long timeoutNs, int ctas,
+                               cudaStream_t s) {
+  void *args[] = {&ctl, &timeoutNs};
+  return cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(barrierProbe), dim3(ctas),
+                                     dim3(kThreads), args, 0, s);
+}
+
+}  // namespace mospb200

@@ -1,0 +1,133 @@
+// engine.h - shared host/device definitions of the sm_100a MOSP engine.
+//
+// The engine is a set of persistent kernels (one CTA group resident per SM,
+// launched cooperatively so that every CTA is co-resident) whose phases are
+// separated by a software grid barrier with a bounded wait. All state a
+// phase hands to the next one lives in the workspace (device memory) or in
+// the control block; per-launch arguments travel as one __grid_constant__
+// parameter block, so a launch needs no host-to-device copy and can be
+// queued back to back with the next one.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+#include "mosp_b200.h"
+
+namespace mospb200 {
+
+using u64 = unsigned long long;
+
+constexpr int kThreads = 512;                 // threads per CTA
+constexpr int kMaxK = MOSP_MAX_OBJECTIVES;    // objectives per launch
+constexpr u64 kInfWord = ~0ULL;               // packed INF (all ones)
+constexpr long long kDistInf = MOSP_DISTANCE_INF;
+constexpr int kLaneRowMax = 32;               // rows above: warp-cooperative
+
+enum EngineMode : int { kModeUpdate = 0, kModeScratch = 1, kModeCombined = 2 };
+
+/// Per-objective arguments of one engine launch.
+struct ObjectiveArgs {
+  const int *outW;       // out-edge weights of this objective [m]
+  const int *inW;        // in-edge weights of this objective [m]
+  long long *dist;       // tree in/out [n]
+  int *parent;           // tree in/out [n]
+  const int *chFrom;     // deleted / weight-increased edges
+  const int *chTo;
+  int nChanged;
+  int parentBits;        // 0: distance-only words
+  u64 noParent;          // all-ones parent field
+  u64 maxDist;           // (n - 1) * maxWeight: no candidate above it
+  u64 delta;             // near-far bucket width (> 0)
+};
+
+/// Control block of one launch: barrier, status and the per-objective list
+/// counters. Counters that change from one iteration to the next live in
+/// rings of three slots (read slot i, write slot i+1, clear slot i+2), so
+/// one grid barrier per iteration suffices.
+struct alignas(128) EngineControl {
+  unsigned arrive;       // barrier arrivals (monotone)
+  unsigned pad0[31];
+  unsigned release;      // barrier epoch released by the last arrival
+  unsigned pad1[31];
+  int status;            // 0 or MOSP_ERR_TIMEOUT (run aborted)
+  int overflow;          // an input distance does not fit the packing
+  int invalid;           // malformed input (ids out of range, cycles)
+  int rounds;            // pointer-jumping rounds
+  int jumpActive[4];
+  int finalGen;          // last stamp generation used
+  int pad2[3];
+  unsigned long long sums[2];  // combined graph: edges, weight sum
+  int candCount[kMaxK];
+  int invalidated[kMaxK];
+  int nearCount[kMaxK][4];
+  int farCount[kMaxK][4];
+  u64 farMinC[kMaxK][4];       // complement of the far-pile minimum
+  int iterations[kMaxK];
+  int epochs[kMaxK];
+  long long pushes[kMaxK];
+};
+
+/// Parameters of one engine launch (passed by value, < 4 KB).
+struct EngineParams {
+  int n, m, K, source;
+  int mode, maxRounds, nHeads, pad;
+  long long timeoutNs;
+  int *genPtr;                 // stamp generation, advanced by every launch
+  const int *outRow, *outCol, *inRow, *inCol;
+  const int *heads;
+  // workspace lists: objective k uses [k * stride, (k + 1) * stride)
+  u64 *packed;
+  int *val, *stamp, *inFar, *cand;
+  int *nearL0, *nearL1, *farL0, *farL1;
+  long long stride;
+  EngineControl *ctl;
+  // combined graph (Steps 2-3)
+  const int *combParents;      // K trees, objective-major
+  int *combDeg, *combRow, *combCol, *combW;
+  long long *blockSums;
+  int combK, combBase;
+  long long combDelta;         // > 0: fixed width; else default
+  int prefTerms[kMaxK];        // L / Pref_i
+  ObjectiveArgs obj[kMaxK];
+};
+
+/// Parameters of the device-graph build.
+struct BuildParams {
+  int n, m, K;
+  long long timeoutNs;
+  const int *outRow, *outCol, *edgeMajorW;
+  int *outW, *inRow, *inCol, *inW;
+  int *cursor;
+  long long *blockSums;
+  EngineControl *ctl;
+};
+
+/// Parameters of the MOSP path-cost kernel.
+struct CostParams {
+  int n, m, KG, source;
+  long long timeoutNs;
+  const int *outRow, *outCol, *outW;  // outW: KG objective-major columns
+  const int *parent;
+  int *edgeOf;
+  int *anc0, *anc1;
+  long long *acc0, *acc1;
+  long long *costs;
+  EngineControl *ctl;
+};
+
+// Host-side launchers (engine.cu). Each returns a cudaError_t of the
+// launch; device-side errors are reported through the control block.
+struct LaunchShape {
+  int engineCtas, buildCtas, costCtas;
+};
+cudaError_t queryLaunchShape(int ctasPerSm, LaunchShape &shape);
+cudaError_t launchEngine(const EngineParams &p, int ctas, cudaStream_t s);
+cudaError_t launchBuild(const BuildParams &p, int ctas, cudaStream_t s);
+cudaError_t launchCosts(const CostParams &p, int ctas, cudaStream_t s);
+cudaError_t launchBarrierProbe(EngineControl *ctl, long long timeoutNs,
+                               int ctas, cudaStream_t s);
+
+}  // namespace mospb200

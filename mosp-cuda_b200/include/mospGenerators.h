@@ -1,0 +1,41 @@
+#ifndef MOSP_B200_GENERATORS_H
+#define MOSP_B200_GENERATORS_H
+
+// Seeded synthetic inputs of the benchmark workloads. The reference measures
+// on SuiteSparse road and geometric graphs (bench/prepare.sh); these
+// generators produce graphs of the same shape in the reference's CSR format
+// (`mospPrep grid|rmat|nearchanges`). No counterpart in the reference.
+
+struct CsrGraph;
+struct ChangeBatch;
+
+/// Road-network shape: a width x height grid whose undirected edges are
+/// kept with probability keep, plus one diagonal shortcut on a
+/// shortcutFraction of the vertices; the largest connected component is
+/// kept and renumbered in row-major order; rows are sorted by head; every
+/// directed edge gets K weights uniform in [wmin, wmax].
+bool generateGridRoad(int width, int height, double keep, double shortcutFraction, int K, int wmin,
+                      int wmax, unsigned seed, CsrGraph &graph);
+
+/// R-MAT: edgeFactor * 2^scale / 2 vertex pairs drawn with quadrant
+/// probabilities a, b, c, d = 1 - a - b - c, symmetrised, self-loops and
+/// duplicates removed (about edgeFactor * 2^scale directed edges); K
+/// weights per directed edge, uniform or log-uniform in [wmin, wmax].
+bool generateRmat(int scale, int edgeFactor, double a, double b, double c, int K, int wmin,
+                  int wmax, bool logUniform, unsigned seed, CsrGraph &graph);
+
+/// Batch on a grid graph with row-major ids (width gridWidth): nIns
+/// insertions of distinct non-edges (u, v) with 1 <= |dx| + |dy| <=
+/// maxManhattan on the grid and weights uniform in [wmin, wmax]; nDel
+/// deletions of distinct existing edges; with safe, deletions that would
+/// disconnect a vertex from source are dropped.
+bool generateNearBatch(const CsrGraph &graph, int gridWidth, int nIns, int nDel, int maxManhattan,
+                       bool safe, unsigned seed, int source, int wmin, int wmax,
+                       ChangeBatch &batch);
+
+/// Remove deletions that would cut a vertex reachable from source off
+/// (the connectivity filter of `mospPrep changes --safe`); returns the
+/// number of filter rounds.
+int filterUnsafeDeletions(const CsrGraph &graph, int source, ChangeBatch &batch);
+
+#endif // MOSP_B200_GENERATORS_H
