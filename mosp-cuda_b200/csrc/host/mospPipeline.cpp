@@ -498,7 +498,12 @@ bool parallelSOSPUpdate(const std::string &originalCsrPrefix, const std::string 
       chTo.push_back(batch.insertTo[i]);
     }
   }
+  // the bound on the distances covers the old tree (original weights) and
+  // the new one (updated weights)
   long long weightSum = 0, maxWeight = 1;
+  for (int e = 0; e < graph.numberOfEdges(); ++e) {
+    maxWeight = std::max(maxWeight, static_cast<long long>(graph.weight(e, k)));
+  }
   for (int e = 0; e < updated.numberOfEdges(); ++e) {
     weightSum += updated.weight(e, k);
     maxWeight = std::max(maxWeight, static_cast<long long>(updated.weight(e, k)));

@@ -178,9 +178,10 @@ def test_distance_only_fallback(ws, ties):
     only, then lowest-id parent recovery (reference src/mospTest.cu:601-700).
     With all weights 2e9 most vertices have two tight parents."""
     W = 2_000_000_000
-    row, col, w = grid_graph(120, 120, 2, W if ties else 2_147_483_647, 0.1, 5, wmin=W if ties else 1)
+    # 320 x 320: 17 parent bits leave 47 for distances < (n - 1) * maxWeight
+    row, col, w = grid_graph(320, 320, 2, W if ties else 2_147_483_647, 0.1, 5, wmin=W if ties else 1)
     g = mb.HostGraph.from_arrays(row, col, w)
-    b = mb.HostBatch.generate(g, 400, seed=6, wmin=W if ties else 1, wmax=W if ties else 2_147_483_647)
+    b = mb.HostBatch.generate(g, 2000, seed=6, wmin=W if ties else 1, wmax=W if ties else 2_147_483_647)
     res = run_update_device(ws, g, b)
     assert all(s.packed_parents == 0 for s in res["stats"])
     assert_matches_oracle(res, g, b)
