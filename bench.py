@@ -217,6 +217,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     wall = time.perf_counter() - wall0
     clock = clocks.stop()
+    phases = {"update": ws.last_phases(0), "combined": ws.last_phases(1)}
     total_ms = float(sum(step_ms))
     if pg:
         t = torch.tensor([total_ms], device="cuda")
@@ -301,7 +302,7 @@ def run_ours(args):
                            "grid_ctas": ws.grid()},
                 "gpu_compute_ms": round(ms_per_step, 4),
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 2 * args.steps,
-                "clocks": clock, "wall_s_timed_loop": round(wall, 4),
+                "clocks": clock, "wall_s_timed_loop": round(wall, 4), "phases_ms": phases,
                 "stats": {"invalidated": [s.invalidated for s in stats], "iterations": [s.iterations for s in stats],
                           "epochs": [s.epochs for s in stats], "pushes": [s.pushes for s in stats],
                           "jump_rounds": stats[0].jump_rounds, "combined_edges": cst.edges,

@@ -147,6 +147,14 @@ int mosp_workspace_enable_timing(mosp_workspace *ws, int on);
 int mosp_workspace_last_timing(mosp_workspace *ws, float *update_ms,
                                float *combined_ms);
 
+/* Device clock (%globaltimer, ns) at the 8 phase boundaries of the last
+ * SOSP-update launch (which = 0) or combined-graph launch (which = 1):
+ * start, trees packed / graph built, roots marked, subtrees flagged,
+ * candidates listed, pull pass done, near-far loop done, results written
+ * (0 for phases a launch does not have). */
+int mosp_workspace_last_phases(mosp_workspace *ws, int which,
+                               unsigned long long *ns);
+
 /* Device buffer number `slot` (0..31) of the workspace, grown to at least
  * `bytes` (contents kept only while it does not grow); freed with the
  * workspace. Lets a caller keep its graph and trees on the device between

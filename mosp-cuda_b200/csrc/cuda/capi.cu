@@ -580,6 +580,14 @@ int mosp_workspace_last_timing(mosp_workspace *ws, float *update_ms, float *comb
   return MOSP_OK;
 }
 
+int mosp_workspace_last_phases(mosp_workspace *ws, int which, unsigned long long *ns) {
+  if (ws == nullptr || ns == nullptr || which < 0 || which > 1) {
+    return fail(MOSP_ERR_INVALID, "invalid phase query");
+  }
+  for (int i = 0; i < 8; ++i) ns[i] = ws->hostCtl[which].phaseNs[i];
+  return MOSP_OK;
+}
+
 int mosp_workspace_grid(mosp_workspace *ws, int *ctas) {
   int st = checkWorkspace(ws);
   if (st != MOSP_OK) return st;

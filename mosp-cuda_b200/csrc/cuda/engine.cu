@@ -129,6 +129,11 @@ __device__ bool gridSync(EngineControl *c, Sync &sync) {
   return sOk != 0;
 }
 
+/// CTA 0 records the time of a phase boundary.
+__device__ __forceinline__ void markPhase(EngineControl *c, int phase) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) c->phaseNs[phase] = globalNs();
+}
+
 /// Reserve one slot of a list: one atomicAdd per group of lanes of the warp
 /// that append to the same counter at the same time.
 __device__ __forceinline__ int warpAppend(int *counter) {
@@ -616,6 +621,7 @@ __global__ void __launch_bounds__(kThreads, 1) sospEngine(const __grid_constant_
   const int *outRow = P.outRow;
   const int *outCol = P.outCol;
 
+  markPhase(c, kPhaseStart);
   if constexpr (Mode == kModeUpdate) {
     // ---- Pack the old trees; ancestors (reference :234-252) ---------------
     for (int k = 0; k < K; ++k) {
@@ -643,6 +649,7 @@ __global__ void __launch_bounds__(kThreads, 1) sospEngine(const __grid_constant_
       }
     }
     if (!gridSync(c, epoch)) return;
+    markPhase(c, kPhasePacked);
 
     // ---- Roots: heads of changed tree edges -------------------------------
     long long changes = 0;
@@ -660,6 +667,7 @@ __global__ void __launch_bounds__(kThreads, 1) sospEngine(const __grid_constant_
       }
     }
     if (!gridSync(c, epoch)) return;
+    markPhase(c, kPhaseRoots);
 
     // ---- Subtree invalidation by pointer jumping (reference :254-291) -----
     // val[v] >= 0: no root on the tree path from v up to (excluding)
@@ -699,6 +707,7 @@ __global__ void __launch_bounds__(kThreads, 1) sospEngine(const __grid_constant_
       }
     }
 
+    markPhase(c, kPhaseJumped);
     // ---- Invalidate; candidates = invalidated + insert heads (:293-313) ---
     for (int k = 0; k < K; ++k) {
       const long long ko = static_cast<long long>(k) * P.stride;
@@ -727,6 +736,7 @@ __global__ void __launch_bounds__(kThreads, 1) sospEngine(const __grid_constant_
       }
     }
     if (!gridSync(c, epoch)) return;
+    markPhase(c, kPhaseCandidates);
 
     // ---- Pull pass over in-edges (reference :315-344) ----------------------
     // The improved candidates form far pile 0; the first iteration of the
@@ -816,8 +826,12 @@ __global__ void __launch_bounds__(kThreads, 1) sospEngine(const __grid_constant_
       }
     }
     if (!gridSync(c, epoch)) return;
+    markPhase(c, kPhasePulled);
     if (!nearFarLoop<Mode>(P, outRow, outCol, sOutWk, epoch, nullptr, genBase)) return;
+    markPhase(c, kPhaseLoop);
     unpackResults<Mode>(P, outRow, outCol, sOutWk, epoch);
+    if (!gridSync(c, epoch)) return;
+    markPhase(c, kPhaseEnd);
   } else {
     scratchOrCombined<Mode>(P, epoch, genBase, sOutWk);
   }
@@ -906,6 +920,7 @@ __device__ void scratchOrCombined(const EngineParams &P, Sync &epoch, int genBas
     outRow = P.combRow;
     outCol = P.combCol;
     if (threadIdx.x == 0) sOutWk[0] = P.combW;
+    markPhase(c, kPhasePacked);
     // fall through to the SSSP from scratch
   }
 
@@ -924,10 +939,14 @@ __device__ void scratchOrCombined(const EngineParams &P, Sync &epoch, int genBas
     }
   }
   if (!gridSync(c, epoch)) return;
+  markPhase(c, kPhasePulled);
   u64 *deltaOverride = nullptr;
   if constexpr (Mode == kModeCombined) deltaOverride = &sCombDelta;
   if (!nearFarLoop<Mode>(P, outRow, outCol, sOutWk, epoch, deltaOverride, genBase)) return;
+  markPhase(c, kPhaseLoop);
   unpackResults<Mode>(P, outRow, outCol, sOutWk, epoch);
+  if (!gridSync(c, epoch)) return;
+  markPhase(c, kPhaseEnd);
 }
 
 // ---------------------------------------------------------------------------

@@ -68,6 +68,20 @@ struct alignas(128) EngineControl {
   int iterations[kMaxK];
   int epochs[kMaxK];
   long long pushes[kMaxK];
+  // %globaltimer at the phase boundaries, written by CTA 0 (see kPhase*)
+  unsigned long long phaseNs[8];
+};
+
+// Phase boundaries recorded in EngineControl::phaseNs.
+enum : int {
+  kPhaseStart = 0,     // kernel start
+  kPhasePacked = 1,    // old trees packed (update) / graph built (combined)
+  kPhaseRoots = 2,     // roots marked
+  kPhaseJumped = 3,    // subtrees flagged by pointer jumping
+  kPhaseCandidates = 4,
+  kPhasePulled = 5,    // pull pass done; near-far loop starts
+  kPhaseLoop = 6,      // near-far loop done
+  kPhaseEnd = 7        // results written
 };
 
 /// Parameters of one engine launch (passed by value, < 4 KB).

@@ -68,6 +68,7 @@ _SIGS = {
     "mosp_workspace_buffer": (_i, [_p, _i, C.c_ulonglong, C.POINTER(_p)]),
     "mosp_workspace_enable_timing": (_i, [_p, _i]),
     "mosp_workspace_last_timing": (_i, [_p, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "mosp_workspace_last_phases": (_i, [_p, _i, C.POINTER(C.c_ulonglong)]),
     "mosp_build_device_graph": (_i, [_p, _i, _i, _i, _p, _p, _p, _p, _p, _p, _p, _p]),
     "mosp_sosp_update": (_i, [_p, _i, _i, _p, _p, _p, _p, _p, _p, _p, _p, _i, _p, _i, _i, _ll, _ll,
                               _p, _p, C.POINTER(SospStats), _p]),
@@ -381,6 +382,20 @@ class Workspace:
         a, b = C.c_float(), C.c_float()
         check(lib().mosp_workspace_last_timing(self._h, C.byref(a), C.byref(b)))
         return a.value, b.value
+
+    PHASES = ("packed", "roots", "jumped", "candidates", "pulled", "loop", "end")
+
+    def last_phases(self, which=0):
+        """Milliseconds spent in each phase of the last update (which=0) or
+        combined (which=1) launch, from the device clock."""
+        ns = (C.c_ulonglong * 8)()
+        check(lib().mosp_workspace_last_phases(self._h, which, ns))
+        out, prev = {}, ns[0]
+        for name, t in zip(self.PHASES, list(ns)[1:]):
+            if t:
+                out[name] = round((t - prev) / 1e6, 4)
+                prev = t
+        return out
 
     def grid(self) -> int:
         c = C.c_int()
