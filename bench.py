@@ -217,7 +217,8 @@ def run_ours(args):
     torch.cuda.synchronize()
     wall = time.perf_counter() - wall0
     clock = clocks.stop()
-    phases = {"update": ws.last_phases(0), "combined": ws.last_phases(1)}
+    phases = {"update": ws.last_phases(0), "combined": ws.last_phases(1),
+              "update_loop": ws.loop_profile(0), "combined_loop": ws.loop_profile(1)}
     total_ms = float(sum(step_ms))
     if pg:
         t = torch.tensor([total_ms], device="cuda")

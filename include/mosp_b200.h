@@ -155,6 +155,13 @@ int mosp_workspace_last_timing(mosp_workspace *ws, float *update_ms,
 int mosp_workspace_last_phases(mosp_workspace *ws, int which,
                                unsigned long long *ns);
 
+/* Near-far loop profile of the last update (which = 0) or combined (1)
+ * launch: time (ns), iterations and list items of the iterations that split
+ * a far pile (index 0) and of the pure push iterations (index 1). */
+int mosp_workspace_loop_profile(mosp_workspace *ws, int which,
+                                unsigned long long *ns, long long *iters,
+                                long long *items);
+
 /* Device buffer number `slot` (0..31) of the workspace, grown to at least
  * `bytes` (contents kept only while it does not grow); freed with the
  * workspace. Lets a caller keep its graph and trees on the device between

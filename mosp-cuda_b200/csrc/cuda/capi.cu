@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <climits>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <string>
@@ -55,7 +56,12 @@ struct mosp_workspace {
   int kCap = 0;
   u64 *packed = nullptr;
   int *val = nullptr, *stamp = nullptr, *inFar = nullptr, *cand = nullptr;
-  int *near0 = nullptr, *near1 = nullptr, *far0 = nullptr, *far1 = nullptr;
+  int *far0 = nullptr, *far1 = nullptr;
+  // near lists (vertex, distance tag): kCap objectives x nearCap entries
+  long long nearCap = 0;
+  int nearK = 0;
+  int *nearV0 = nullptr, *nearV1 = nullptr;
+  u64 *nearD0 = nullptr, *nearD1 = nullptr;
   int *gen = nullptr;  // device stamp generation
   bool dirty = false;  // an aborted run may have left inFar/stamp set
   // control blocks
@@ -100,19 +106,30 @@ int deviceAlloc(T **ptr, size_t count) {
   return MOSP_OK;
 }
 
+void releaseNear(mosp_workspace *ws) {
+  for (void *p : {static_cast<void *>(ws->nearV0), static_cast<void *>(ws->nearV1),
+                  static_cast<void *>(ws->nearD0), static_cast<void *>(ws->nearD1)}) {
+    if (p) cudaFree(p);
+  }
+  ws->nearV0 = ws->nearV1 = nullptr;
+  ws->nearD0 = ws->nearD1 = nullptr;
+  ws->nearCap = 0;
+  ws->nearK = 0;
+}
+
 void releaseLists(mosp_workspace *ws) {
   for (void *p : {static_cast<void *>(ws->packed), static_cast<void *>(ws->val),
                   static_cast<void *>(ws->stamp), static_cast<void *>(ws->inFar),
-                  static_cast<void *>(ws->cand), static_cast<void *>(ws->near0),
-                  static_cast<void *>(ws->near1), static_cast<void *>(ws->far0),
+                  static_cast<void *>(ws->cand), static_cast<void *>(ws->far0),
                   static_cast<void *>(ws->far1)}) {
     if (p) cudaFree(p);
   }
   ws->packed = nullptr;
   ws->val = ws->stamp = ws->inFar = ws->cand = nullptr;
-  ws->near0 = ws->near1 = ws->far0 = ws->far1 = nullptr;
+  ws->far0 = ws->far1 = nullptr;
   ws->nCap = 0;
   ws->kCap = 0;
+  releaseNear(ws);
 }
 
 int ensureShape(mosp_workspace *ws) {
@@ -133,6 +150,26 @@ int ensureShape(mosp_workspace *ws) {
   return MOSP_OK;
 }
 
+/// Near lists of K objectives with room for n + m entries each: one
+/// iteration appends at most one entry per relaxation (<= m) and a split
+/// at most one per far-pile vertex (<= n).
+int reserveNear(mosp_workspace *ws, long long n, long long m, int K) {
+  const long long need = n + m + 64;
+  if (need <= ws->nearCap && K <= ws->nearK && ws->nearV0 != nullptr) return MOSP_OK;
+  const long long cap = std::max(need, ws->nearCap);
+  const int kk = std::max(K, ws->nearK);
+  releaseNear(ws);
+  const size_t total = static_cast<size_t>(cap) * kk;
+  int st = MOSP_OK;
+  if ((st = deviceAlloc(&ws->nearV0, total)) != MOSP_OK) return st;
+  if ((st = deviceAlloc(&ws->nearV1, total)) != MOSP_OK) return st;
+  if ((st = deviceAlloc(&ws->nearD0, total)) != MOSP_OK) return st;
+  if ((st = deviceAlloc(&ws->nearD1, total)) != MOSP_OK) return st;
+  ws->nearCap = cap;
+  ws->nearK = kk;
+  return MOSP_OK;
+}
+
 int reserveLists(mosp_workspace *ws, long long n, int K) {
   if (n <= ws->nCap && K <= ws->kCap) return MOSP_OK;
   const long long newN = std::max(n, ws->nCap);
@@ -141,8 +178,7 @@ int reserveLists(mosp_workspace *ws, long long n, int K) {
   const size_t total = static_cast<size_t>(newN) * newK;
   int st = MOSP_OK;
   if ((st = deviceAlloc(&ws->packed, total)) != MOSP_OK) return st;
-  for (int **p : {&ws->val, &ws->stamp, &ws->inFar, &ws->cand, &ws->near0, &ws->near1,
-                  &ws->far0, &ws->far1}) {
+  for (int **p : {&ws->val, &ws->stamp, &ws->inFar, &ws->cand, &ws->far0, &ws->far1}) {
     if ((st = deviceAlloc(p, total)) != MOSP_OK) {
       releaseLists(ws);
       return st;
@@ -224,7 +260,19 @@ void setObjective(ObjectiveArgs &o, int bits, u64 maxDist, long long delta) {
   o.delta = static_cast<u64>(delta);
 }
 
+/// Tuning switches of the engine (EngineParams::flags) from the
+/// environment variable MOSP_ENGINE_FLAGS (decimal); results do not depend
+/// on them.
+int engineFlags() {
+  static const int flags = [] {
+    const char *e = std::getenv("MOSP_ENGINE_FLAGS");
+    return e != nullptr ? std::atoi(e) : 0;
+  }();
+  return flags;
+}
+
 void fillLists(EngineParams &p, mosp_workspace *ws, int block) {
+  p.flags = engineFlags();
   p.timeoutNs = ws->timeoutNs;
   p.genPtr = ws->gen;
   p.packed = ws->packed;
@@ -232,8 +280,11 @@ void fillLists(EngineParams &p, mosp_workspace *ws, int block) {
   p.stamp = ws->stamp;
   p.inFar = ws->inFar;
   p.cand = ws->cand;
-  p.nearL0 = ws->near0;
-  p.nearL1 = ws->near1;
+  p.nearV0 = ws->nearV0;
+  p.nearV1 = ws->nearV1;
+  p.nearD0 = ws->nearD0;
+  p.nearD1 = ws->nearD1;
+  p.strideNear = ws->nearCap;
   p.farL0 = ws->far0;
   p.farL1 = ws->far1;
   p.stride = ws->nCap;
@@ -348,6 +399,7 @@ int prepareUpdate(mosp_workspace *ws, const UpdateArgs &a, EngineParams &p, int 
   }
   int st = reserveLists(ws, a.n, a.K);
   if (st != MOSP_OK) return st;
+  if ((st = reserveNear(ws, a.n, a.m, a.K)) != MOSP_OK) return st;
   std::memset(&p, 0, sizeof(p));
   p.n = a.n;
   p.m = a.m;
@@ -399,6 +451,7 @@ int prepareCombined(mosp_workspace *ws, int n, int K, const int *d_parents, cons
   int st = reserveLists(ws, n, 1);
   if (st != MOSP_OK) return st;
   if ((st = reserveCombined(ws, n, K)) != MOSP_OK) return st;
+  if ((st = reserveNear(ws, n, static_cast<long long>(n) * K, 1)) != MOSP_OK) return st;
   std::memset(&p, 0, sizeof(p));
   p.n = n;
   p.K = 1;
@@ -588,6 +641,18 @@ int mosp_workspace_last_phases(mosp_workspace *ws, int which, unsigned long long
   return MOSP_OK;
 }
 
+int mosp_workspace_loop_profile(mosp_workspace *ws, int which, unsigned long long *ns,
+                                long long *iters, long long *items) {
+  if (ws == nullptr || which < 0 || which > 1) return fail(MOSP_ERR_INVALID, "invalid query");
+  const EngineControl &c = ws->hostCtl[which];
+  for (int q = 0; q < 2; ++q) {
+    if (ns) ns[q] = c.loopNs[q];
+    if (iters) iters[q] = c.loopIters[q];
+    if (items) items[q] = c.loopItems[q];
+  }
+  return MOSP_OK;
+}
+
 int mosp_workspace_grid(mosp_workspace *ws, int *ctas) {
   int st = checkWorkspace(ws);
   if (st != MOSP_OK) return st;
@@ -700,6 +765,7 @@ int mosp_sosp_from_scratch(mosp_workspace *ws, int n, int m, const int *d_out_ro
     return fail(MOSP_ERR_INVALID, "Error: invalid SSSP arguments.");
   }
   if ((st = reserveLists(ws, n, 1)) != MOSP_OK) return st;
+  if ((st = reserveNear(ws, n, m, 1)) != MOSP_OK) return st;
   int bits = 0;
   u64 maxDist = 0;
   if ((st = choosePacking(n, max_weight, bits, maxDist)) != MOSP_OK) return st;

@@ -197,46 +197,174 @@ struct LoopShared {
 enum : int { kDone = 0, kPush = 1, kSplit = 2 };
 
 // ---------------------------------------------------------------------------
-// Relaxation of one out-edge (push)
+// Per-CTA staging of list appends
+//
+// Every append of an iteration (next near list, far piles) goes to a
+// shared-memory buffer first: a shared atomic per warp group gives the slot
+// and the rank within the destination list. At the end of the iteration the
+// CTA reserves one range per list with a single global atomic and copies
+// its entries out, so the same-address global counters see one atomic per
+// CTA and list instead of one per warp group on the relaxation's critical
+// path. Entries that do not fit the buffer take the direct global path.
 // ---------------------------------------------------------------------------
-template <int Mode>
-__device__ __forceinline__ void relaxEdge(const EngineParams &P, const int *outCol,
-                                          const int *outW, int k, int u, u64 du,
-                                          int e, const LoopShared &L, int wrSlot,
-                                          int *nearW, int gen) {
-  const ObjectiveArgs &O = P.obj[k];
-  const int w = ldGraph<Mode>(outCol + e);
-  if (w == P.source) return;
-  const u64 nd = du + static_cast<u64>(ldGraph<Mode>(outW + e));
-  if (nd > O.maxDist) return;  // never shortest; would not fit the word
-  const Pk pk = pkOf(O);
-  const u64 cand = pk.pack(nd, u);
-  const long long base = static_cast<long long>(k) * P.stride;
-  u64 *pw = P.packed + base + w;
-  if (cand >= __ldcg(pw)) return;
-  const u64 old = atomicMin(pw, cand);
-  if (nd >= pk.dist(old)) return;  // distance did not improve
-  if (nd < L.thr[k]) {
-    if (atomicExch(P.stamp + base + w, gen) != gen) {
-      const int idx = warpAppend(&P.ctl->nearCount[k][wrSlot]);
-      nearW[base + idx] = w;
-    }
-  } else if (atomicExch(P.inFar + base + w, 1) == 0) {
-    const int fs = L.fs[k];
-    const int idx = warpAppend(&P.ctl->farCount[k][fs]);
-    (L.fp[k] == 0 ? P.farL0 : P.farL1)[base + idx] = w;
-    warpMinInto(&P.ctl->farMinC[k][fs], nd);
+constexpr int kStage = 4096;
+
+struct StageHeader {
+  int total;                   // staging attempts (may exceed kStage)
+  int pad;
+  int count[2 * kMaxK];        // staged entries per list (near k, far K+k)
+  int base[2 * kMaxK];         // global start of this CTA's range
+  u64 farMin[kMaxK];           // minimum distance appended to far (plain)
+  long long expanded[kMaxK];   // non-stale expansions (statistics)
+};
+
+struct StageEntry {
+  int v;
+  int meta;                    // list << 16 | rank
+  u64 d;
+};
+
+constexpr size_t kStageHeaderBytes = (sizeof(StageHeader) + 15) / 16 * 16;
+constexpr size_t kStageBytes = kStageHeaderBytes + kStage * sizeof(StageEntry);
+
+__device__ __forceinline__ StageHeader &stageHeader() {
+  extern __shared__ __align__(16) unsigned char dynSmem[];
+  return *reinterpret_cast<StageHeader *>(dynSmem);
+}
+
+__device__ __forceinline__ StageEntry *stageEntries() {
+  extern __shared__ __align__(16) unsigned char dynSmem[];
+  return reinterpret_cast<StageEntry *>(dynSmem + kStageHeaderBytes);
+}
+
+/// Destination of list l in this iteration: near list of objective l (l <
+/// K) or the far pile objective l - K appends to (the current pile while it
+/// pushes, the other pile while its pile is split).
+struct Target {
+  int *counter;
+  int *v;
+  u64 *d;
+  u64 *minC;
+};
+
+__device__ __forceinline__ Target listTarget(const EngineParams &P, const LoopShared &L, int l,
+                                             int wrSlot, int *nearWV, u64 *nearWD) {
+  const int K = P.K;
+  if (l < K) {
+    const long long kn = static_cast<long long>(l) * P.strideNear;
+    return Target{&P.ctl->nearCount[l][wrSlot], nearWV + kn, nearWD + kn, nullptr};
   }
+  const int k = l - K;
+  const long long ko = static_cast<long long>(k) * P.stride;
+  if (L.mode[k] == kSplit) {
+    const int s = (L.fs[k] + 1) % 3;
+    return Target{&P.ctl->farCount[k][s], (L.fp[k] == 0 ? P.farL1 : P.farL0) + ko, nullptr,
+                  &P.ctl->farMinC[k][s]};
+  }
+  const int s = L.fs[k];
+  return Target{&P.ctl->farCount[k][s], (L.fp[k] == 0 ? P.farL0 : P.farL1) + ko, nullptr,
+                &P.ctl->farMinC[k][s]};
+}
+
+/// Append (v, d) to list l (far lists: d only feeds the pile minimum).
+__device__ __forceinline__ void stageAppend(const EngineParams &P, const LoopShared &L, int l,
+                                            int v, u64 d, int wrSlot, int *nearWV, u64 *nearWD) {
+  StageHeader &H = stageHeader();
+  StageEntry *E = stageEntries();
+  const unsigned lane = laneId();
+  const unsigned lt = (1u << lane) - 1u;
+  const unsigned mask = __activemask();
+  const unsigned peers = __match_any_sync(mask, l);
+  const int leader = __ffs(peers) - 1;
+  int slotBase = 0;
+  if (static_cast<int>(lane) == leader) slotBase = atomicAdd(&H.total, __popc(peers));
+  slotBase = __shfl_sync(peers, slotBase, leader);
+  const int slot = slotBase + __popc(peers & lt);
+  const bool staged = slot < kStage;
+  const unsigned stagedMask = __ballot_sync(peers, staged);
+  int rankBase = 0;
+  if (static_cast<int>(lane) == leader && stagedMask != 0) {
+    rankBase = atomicAdd(&H.count[l], __popc(stagedMask));
+  }
+  rankBase = __shfl_sync(peers, rankBase, leader);
+  if (l >= P.K) {
+    // far pile minimum of this CTA (shared), reduced over the group first
+    const unsigned hi = static_cast<unsigned>(d >> 32), lo = static_cast<unsigned>(d);
+    const unsigned mhi = __reduce_min_sync(peers, hi);
+    const unsigned mlo = __reduce_min_sync(peers, hi == mhi ? lo : 0xffffffffu);
+    if (static_cast<int>(lane) == leader) {
+      atomicMin(&H.farMin[l - P.K], (static_cast<u64>(mhi) << 32) | mlo);
+    }
+  }
+  if (staged) {
+    E[slot] = StageEntry{v, (l << 16) | (rankBase + __popc(stagedMask & lt)), d};
+  } else {
+    const Target t = listTarget(P, L, l, wrSlot, nearWV, nearWD);
+    const int idx = warpAppend(t.counter);
+    t.v[idx] = v;
+    if (t.d != nullptr) t.d[idx] = d;
+  }
+}
+
+/// End of an iteration: reserve every list's range once per CTA, copy the
+/// staged entries out, fold the far minima and the statistics.
+__device__ void flushStage(const EngineParams &P, const LoopShared &L, int wrSlot, int *nearWV,
+                           u64 *nearWD) {
+  StageHeader &H = stageHeader();
+  StageEntry *E = stageEntries();
+  const int K = P.K;
+  __syncthreads();
+  const int t = threadIdx.x;
+  if (t < 2 * K && H.count[t] > 0) {
+    H.base[t] = atomicAdd(listTarget(P, L, t, wrSlot, nearWV, nearWD).counter, H.count[t]);
+  }
+  if (t < K && H.farMin[t] != kInfWord) {
+    atomicMax(listTarget(P, L, K + t, wrSlot, nearWV, nearWD).minC, ~H.farMin[t]);
+  }
+  if (t < K && H.expanded[t] != 0) {
+    atomicAdd(reinterpret_cast<unsigned long long *>(&P.ctl->pushes[t]),
+              static_cast<unsigned long long>(H.expanded[t]));
+  }
+  __syncthreads();
+  const int total = H.total < kStage ? H.total : kStage;
+  for (int i = t; i < total; i += blockDim.x) {
+    const StageEntry e = E[i];
+    const int l = e.meta >> 16;
+    const Target tg = listTarget(P, L, l, wrSlot, nearWV, nearWD);
+    const int idx = H.base[l] + (e.meta & 0xffff);
+    tg.v[idx] = e.v;
+    if (tg.d != nullptr) tg.d[idx] = e.d;
+  }
+}
+
+/// Lane of the warp whose edge range holds edge slot s: the number of
+/// lanes whose inclusive edge count is <= s (binary search by shuffles).
+__device__ __forceinline__ int slotOwner(int incl, int s) {
+  int lo = 0;
+#pragma unroll
+  for (int step = 16; step >= 1; step >>= 1) {
+    const int probe = __shfl_sync(kFull, incl, lo + step - 1);
+    if (probe <= s) lo += step;
+  }
+  return lo;
 }
 
 // ---------------------------------------------------------------------------
 // Near-far loop shared by every mode
+//
+// Near lists carry (vertex, distance) pairs: an entry is stale when the
+// vertex's word has a smaller distance by the time it is read, and is then
+// skipped (a newer entry exists). Every strict improvement appends exactly
+// one entry, so no claim atomic is needed and a list never holds more
+// entries than the relaxations of one iteration (<= m) plus the far pile
+// (<= n). Far piles keep one entry per vertex (inFar flag).
 // ---------------------------------------------------------------------------
 template <int Mode>
 __device__ bool nearFarLoop(const EngineParams &P, const int *outRow,
                             const int *outCol, const int *const *outWk,
                             Sync &epoch, u64 *deltaOverride, int genBase) {
   __shared__ LoopShared L;
+  StageHeader &H = stageHeader();
   EngineControl *c = P.ctl;
   const int K = P.K;
   const unsigned lane = laneId();
@@ -248,7 +376,6 @@ __device__ bool nearFarLoop(const EngineParams &P, const int *outRow,
   u64 thr = 0;
   int fp = 0, fs = 0;
   int iters = 0, epochs = 0;
-  long long pushes = 0;
   u64 delta = 1;
   if (warp == 0 && static_cast<int>(lane) < K) {
     delta = P.obj[lane].delta;
@@ -256,8 +383,17 @@ __device__ bool nearFarLoop(const EngineParams &P, const int *outRow,
   }
 
   int it = 0;
+  unsigned long long profNs[2] = {0, 0};
+  long long profIters[2] = {0, 0}, profItems[2] = {0, 0};
   for (;; ++it) {
     const int rdSlot = it % 3, wrSlot = (it + 1) % 3, clrSlot = (it + 2) % 3;
+    const unsigned long long itStart = globalNs();
+    if (threadIdx.x < 2 * kMaxK) H.count[threadIdx.x] = 0;
+    if (threadIdx.x < kMaxK) {
+      H.farMin[threadIdx.x] = kInfWord;
+      H.expanded[threadIdx.x] = 0;
+    }
+    if (threadIdx.x == 0) H.total = 0;
     if (warp == 0) {
       const int k = static_cast<int>(lane);
       const bool act = k < K;
@@ -283,7 +419,6 @@ __device__ bool nearFarLoop(const EngineParams &P, const int *outRow,
           }
         }
       }
-      // exclusive prefix of items over the objectives
       long long incl = items;
 #pragma unroll
       for (int off = 1; off < 32; off <<= 1) {
@@ -309,7 +444,6 @@ __device__ bool nearFarLoop(const EngineParams &P, const int *outRow,
         }
         if (mode == kPush) {
           ++iters;
-          pushes += items;
         } else if (mode == kSplit) {
           ++epochs;
           fp ^= 1;           // takes effect after this iteration
@@ -321,9 +455,10 @@ __device__ bool nearFarLoop(const EngineParams &P, const int *outRow,
     const long long total = L.total;
     if (total == 0) break;
 
-    const int gen = genBase + 1 + it;
-    const int *nearR = (it & 1) ? P.nearL1 : P.nearL0;
-    int *nearW = (it & 1) ? P.nearL0 : P.nearL1;
+    const int *nearRV = (it & 1) ? P.nearV1 : P.nearV0;
+    const u64 *nearRD = (it & 1) ? P.nearD1 : P.nearD0;
+    int *nearWV = (it & 1) ? P.nearV0 : P.nearV1;
+    u64 *nearWD = (it & 1) ? P.nearD0 : P.nearD1;
 
     for (long long base = gwarp * 32; base < total; base += nwarps * 32) {
       const long long j = base + lane;
@@ -337,69 +472,143 @@ __device__ bool nearFarLoop(const EngineParams &P, const int *outRow,
       const long long ko = static_cast<long long>(k) * P.stride;
 
       if (mode == kSplit) {
-        // far pile entry: back to the near list below the new threshold
+        // far pile entry: to the near list below the new threshold
         const int v = __ldcg((L.fp[k] == 0 ? P.farL0 : P.farL1) + ko + i);
         const u64 word = __ldcg(P.packed + ko + v);
-        const Pk pk = pkOf(P.obj[k]);
-        const u64 d = word == kInfWord ? kInfWord : pk.dist(word);
+        const u64 d = word == kInfWord ? kInfWord : pkOf(P.obj[k]).dist(word);
         if (d < L.thr[k]) {
           P.inFar[ko + v] = 0;
-          if (atomicExch(P.stamp + ko + v, gen) != gen) {
-            const int idx = warpAppend(&c->nearCount[k][wrSlot]);
-            nearW[ko + idx] = v;
-          }
+          stageAppend(P, L, k, v, d, wrSlot, nearWV, nearWD);
         } else {
-          const int nfs = (L.fs[k] + 1) % 3;
-          const int idx = warpAppend(&c->farCount[k][nfs]);
-          (L.fp[k] == 0 ? P.farL1 : P.farL0)[ko + idx] = v;
-          warpMinInto(&c->farMinC[k][nfs], d);
+          stageAppend(P, L, K + k, v, d, wrSlot, nearWV, nearWD);
         }
       }
 
-      // push: expand the near-list vertex of this lane
-      int u = -1, beg = 0, end = 0;
+      // push: one non-stale near entry per lane, edges spread over the warp
+      int u = -1, beg = 0, deg = 0;
       u64 du = 0;
       if (mode == kPush) {
-        u = __ldcg(nearR + ko + i);
+        const long long kn = static_cast<long long>(k) * P.strideNear;
+        u = __ldcg(nearRV + kn + i);
+        const u64 tag = __ldcg(nearRD + kn + i);
         const u64 word = __ldcg(P.packed + ko + u);
-        if (word != kInfWord) {
-          du = pkOf(P.obj[k]).dist(word);
+        if (word != kInfWord && pkOf(P.obj[k]).dist(word) == tag) {
+          du = tag;
           beg = ldGraph<Mode>(outRow + u);
-          end = ldGraph<Mode>(outRow + u + 1);
+          deg = ldGraph<Mode>(outRow + u + 1) - beg;
+          atomicAdd(reinterpret_cast<unsigned long long *>(&H.expanded[k]), 1ULL);
         }
       }
-      const int deg = end - beg;
-      unsigned big = __ballot_sync(kFull, deg > kLaneRowMax);
-      if (deg > 0 && deg <= kLaneRowMax) {
-        const int *w = outWk[k];
-        for (int e = beg; e < end; ++e) {
-          relaxEdge<Mode>(P, outCol, w, k, u, du, e, L, wrSlot, nearW, gen);
-        }
-      }
-      while (big != 0) {
-        const int src = __ffs(big) - 1;
-        big &= big - 1;
+      if (__ballot_sync(kFull, deg > 0) == 0) continue;
+      // rows above 2^20 edges: whole-warp striding, one row at a time
+      unsigned huge = __ballot_sync(kFull, deg > (1 << 20));
+      while (huge != 0) {
+        const int src = __ffs(huge) - 1;
+        huge &= huge - 1;
         const int kb = __shfl_sync(kFull, k, src);
         const int ub = __shfl_sync(kFull, u, src);
         const u64 db = __shfl_sync(kFull, du, src);
         const int bb = __shfl_sync(kFull, beg, src);
-        const int eb = __shfl_sync(kFull, end, src);
-        const int *w = outWk[kb];
+        const int eb = bb + __shfl_sync(kFull, deg, src);
+        const ObjectiveArgs &O = P.obj[kb];
+        const Pk pk = pkOf(O);
+        const long long kob = static_cast<long long>(kb) * P.stride;
         for (int e = bb + static_cast<int>(lane); e < eb; e += 32) {
-          relaxEdge<Mode>(P, outCol, w, kb, ub, db, e, L, wrSlot, nearW, gen);
+          const int w = ldGraph<Mode>(outCol + e);
+          const u64 nd = db + static_cast<u64>(ldGraph<Mode>(outWk[kb] + e));
+          if (w == P.source || nd > O.maxDist) continue;
+          const u64 old = atomicMin(P.packed + kob + w, pk.pack(nd, ub));
+          if (nd >= pk.dist(old)) continue;
+          if (nd < L.thr[kb]) {
+            stageAppend(P, L, kb, w, nd, wrSlot, nearWV, nearWD);
+          } else if (atomicExch(P.inFar + kob + w, 1) == 0) {
+            stageAppend(P, L, K + kb, w, nd, wrSlot, nearWV, nearWD);
+          }
+        }
+      }
+      if (deg > (1 << 20)) deg = 0;
+      int incl = deg;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const int o = __shfl_up_sync(kFull, incl, off);
+        if (static_cast<int>(lane) >= off) incl += o;
+      }
+      const int edges = __shfl_sync(kFull, incl, 31);
+      const int excl = incl - deg;
+      for (int s0 = 0; s0 < edges; s0 += 64) {
+        // two edge slots per lane, their loads and atomics overlapped
+        int sl[2], kk[2], uu[2], ee[2], ww[2], wt[2];
+        u64 dd[2], nd[2], old[2];
+        bool act[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          sl[h] = s0 + 32 * h + static_cast<int>(lane);
+          const int o = slotOwner(incl, sl[h]);
+          kk[h] = __shfl_sync(kFull, k, o);
+          uu[h] = __shfl_sync(kFull, u, o);
+          dd[h] = __shfl_sync(kFull, du, o);
+          ee[h] = __shfl_sync(kFull, beg, o) + sl[h] - __shfl_sync(kFull, excl, o);
+          act[h] = sl[h] < edges;
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          ww[h] = act[h] ? ldGraph<Mode>(outCol + ee[h]) : 0;
+          wt[h] = act[h] ? ldGraph<Mode>(outWk[kk[h]] + ee[h]) : 0;
+        }
+        u64 cw[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          nd[h] = dd[h] + static_cast<u64>(wt[h]);
+          act[h] = act[h] && ww[h] != P.source && nd[h] <= P.obj[kk[h]].maxDist;
+          cw[h] = pkOf(P.obj[kk[h]]).pack(nd[h], uu[h]);
+        }
+        if (P.flags & kFlagPrecheck) {
+          u64 cur[2];
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            cur[h] = act[h] ? __ldcg(P.packed + static_cast<long long>(kk[h]) * P.stride + ww[h]) : 0;
+          }
+#pragma unroll
+          for (int h = 0; h < 2; ++h) act[h] = act[h] && cw[h] < cur[h];
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          old[h] = act[h] ? atomicMin(P.packed + static_cast<long long>(kk[h]) * P.stride + ww[h], cw[h])
+                          : 0;
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          if (!act[h] || nd[h] >= pkOf(P.obj[kk[h]]).dist(old[h])) continue;
+          if (nd[h] < L.thr[kk[h]]) {
+            stageAppend(P, L, kk[h], ww[h], nd[h], wrSlot, nearWV, nearWD);
+          } else if (atomicExch(P.inFar + static_cast<long long>(kk[h]) * P.stride + ww[h], 1) == 0) {
+            stageAppend(P, L, K + kk[h], ww[h], nd[h], wrSlot, nearWV, nearWD);
+          }
         }
       }
     }
+    flushStage(P, L, wrSlot, nearWV, nearWD);
     if (!gridSync(c, epoch)) return false;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      bool split = false;
+      for (int k = 0; k < K; ++k) split |= L.mode[k] == kSplit;
+      profNs[split ? 0 : 1] += globalNs() - itStart;
+      profIters[split ? 0 : 1] += 1;
+      profItems[split ? 0 : 1] += total;
+    }
   }
 
   if (blockIdx.x == 0 && warp == 0 && static_cast<int>(lane) < K) {
     c->iterations[lane] = iters;
     c->epochs[lane] = epochs;
-    c->pushes[lane] = pushes;
     if (lane == 0) {
       c->finalGen = genBase + 1 + it;
       *P.genPtr = genBase + 1 + it;
+      for (int q = 0; q < 2; ++q) {
+        c->loopNs[q] = profNs[q];
+        c->loopIters[q] = profIters[q];
+        c->loopItems[q] = profItems[q];
+      }
     }
   }
   return true;
@@ -1142,9 +1351,15 @@ __global__ void barrierProbe(EngineControl *c, long long timeoutNs) {
 }
 
 template <typename Kernel>
-cudaError_t ctasFor(Kernel kernel, int sms, int ctasPerSm, int &ctas) {
+cudaError_t ctasFor(Kernel kernel, int sms, int ctasPerSm, int &ctas, size_t smem = 0) {
   int perSm = 0;
-  cudaError_t err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, kThreads, 0);
+  if (smem > 0) {
+    cudaError_t a = cudaFuncSetAttribute(reinterpret_cast<const void *>(kernel),
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (a != cudaSuccess) return a;
+  }
+  cudaError_t err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, kThreads, smem);
   if (err != cudaSuccess) return err;
   if (perSm < 1) return cudaErrorInvalidConfiguration;
   if (ctasPerSm > 0 && ctasPerSm < perSm) perSm = ctasPerSm;
@@ -1162,9 +1377,9 @@ cudaError_t queryLaunchShape(int ctasPerSm, LaunchShape &shape) {
   if (err != cudaSuccess) return err;
   if (!coop) return cudaErrorNotSupported;
   int a = 0, b = 0, d = 0, e = 0;
-  if ((err = ctasFor(sospEngine<kModeUpdate>, sms, ctasPerSm, a)) != cudaSuccess) return err;
-  if ((err = ctasFor(sospEngine<kModeScratch>, sms, ctasPerSm, b)) != cudaSuccess) return err;
-  if ((err = ctasFor(sospEngine<kModeCombined>, sms, ctasPerSm, d)) != cudaSuccess) return err;
+  if ((err = ctasFor(sospEngine<kModeUpdate>, sms, ctasPerSm, a, kStageBytes)) != cudaSuccess) return err;
+  if ((err = ctasFor(sospEngine<kModeScratch>, sms, ctasPerSm, b, kStageBytes)) != cudaSuccess) return err;
+  if ((err = ctasFor(sospEngine<kModeCombined>, sms, ctasPerSm, d, kStageBytes)) != cudaSuccess) return err;
   shape.engineCtas = a < b ? (a < d ? a : d) : (b < d ? b : d);
   if ((err = ctasFor(buildGraph, sms, ctasPerSm, e)) != cudaSuccess) return err;
   shape.buildCtas = e;
@@ -1181,7 +1396,7 @@ cudaError_t launchEngine(const EngineParams &p, int ctas, cudaStream_t s) {
     case kModeScratch: fn = reinterpret_cast<const void *>(sospEngine<kModeScratch>); break;
     default: fn = reinterpret_cast<const void *>(sospEngine<kModeCombined>); break;
   }
-  return cudaLaunchCooperativeKernel(fn, dim3(ctas), dim3(kThreads), args, 0, s);
+  return cudaLaunchCooperativeKernel(fn, dim3(ctas), dim3(kThreads), args, kStageBytes, s);
 }
 
 cudaError_t launchBuild(const BuildParams &p, int ctas, cudaStream_t s) {

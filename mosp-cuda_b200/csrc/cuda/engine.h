@@ -70,6 +70,16 @@ struct alignas(128) EngineControl {
   long long pushes[kMaxK];
   // %globaltimer at the phase boundaries, written by CTA 0 (see kPhase*)
   unsigned long long phaseNs[8];
+  // near-far loop profile, written by CTA 0: time and items of iterations
+  // that split a far pile ([0]) and of pure push iterations ([1])
+  unsigned long long loopNs[2];
+  long long loopIters[2];
+  long long loopItems[2];
+};
+
+// EngineParams::flags (tuning switches; results do not depend on them)
+enum : int {
+  kFlagPrecheck = 1  // read the word before the atomicMin of a relaxation
 };
 
 // Phase boundaries recorded in EngineControl::phaseNs.
@@ -87,16 +97,19 @@ enum : int {
 /// Parameters of one engine launch (passed by value, < 4 KB).
 struct EngineParams {
   int n, m, K, source;
-  int mode, maxRounds, nHeads, pad;
+  int mode, maxRounds, nHeads, flags;
   long long timeoutNs;
   int *genPtr;                 // stamp generation, advanced by every launch
   const int *outRow, *outCol, *inRow, *inCol;
   const int *heads;
-  // workspace lists: objective k uses [k * stride, (k + 1) * stride)
+  // workspace lists: objective k uses [k * stride, (k + 1) * stride) of the
+  // per-vertex arrays and [k * strideNear, ...) of the near lists
   u64 *packed;
   int *val, *stamp, *inFar, *cand;
-  int *nearL0, *nearL1, *farL0, *farL1;
-  long long stride;
+  int *farL0, *farL1;
+  int *nearV0, *nearV1;        // near lists: vertices
+  u64 *nearD0, *nearD1;        // near lists: distance when appended
+  long long stride, strideNear;
   EngineControl *ctl;
   // combined graph (Steps 2-3)
   const int *combParents;      // K trees, objective-major

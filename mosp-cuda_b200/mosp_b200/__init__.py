@@ -69,6 +69,7 @@ _SIGS = {
     "mosp_workspace_enable_timing": (_i, [_p, _i]),
     "mosp_workspace_last_timing": (_i, [_p, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "mosp_workspace_last_phases": (_i, [_p, _i, C.POINTER(C.c_ulonglong)]),
+    "mosp_workspace_loop_profile": (_i, [_p, _i, C.POINTER(C.c_ulonglong), _llp, _llp]),
     "mosp_build_device_graph": (_i, [_p, _i, _i, _i, _p, _p, _p, _p, _p, _p, _p, _p]),
     "mosp_sosp_update": (_i, [_p, _i, _i, _p, _p, _p, _p, _p, _p, _p, _p, _i, _p, _i, _i, _ll, _ll,
                               _p, _p, C.POINTER(SospStats), _p]),
@@ -396,6 +397,15 @@ class Workspace:
                 out[name] = round((t - prev) / 1e6, 4)
                 prev = t
         return out
+
+    def loop_profile(self, which=0):
+        """Near-far loop of the last launch: {split|push: (ms, iterations,
+        items)}."""
+        ns = (C.c_ulonglong * 2)()
+        it = (C.c_longlong * 2)()
+        items = (C.c_longlong * 2)()
+        check(lib().mosp_workspace_loop_profile(self._h, which, ns, it, items))
+        return {name: (round(ns[q] / 1e6, 4), it[q], items[q]) for q, name in enumerate(("split", "push"))}
 
     def grid(self) -> int:
         c = C.c_int()
