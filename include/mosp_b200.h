@@ -157,7 +157,9 @@ int mosp_workspace_last_phases(mosp_workspace *ws, int which,
 
 /* Near-far loop profile of the last update (which = 0) or combined (1)
  * launch: time (ns), iterations and list items of the iterations that split
- * a far pile (index 0) and of the pure push iterations (index 1). */
+ * a far pile (index 0) and of the pure push iterations (index 1); ns[2..6]
+ * (ns has 7 entries) split the push iterations of CTA 0 into decision step,
+ * own items, wait for the CTA's other warps, list flush and grid barrier. */
 int mosp_workspace_loop_profile(mosp_workspace *ws, int which,
                                 unsigned long long *ns, long long *iters,
                                 long long *items);
@@ -314,6 +316,13 @@ int mosp_update_host(mosp_workspace *ws, int n, int KG, int m,
  * are unbounded, src/sospUpdateGpu.cu:644-649). */
 int mosp_debug_barrier_timeout(mosp_workspace *ws, long long timeout_ms,
                                int *device_status);
+
+/* Device time per grid barrier of the persistent kernels' launch shape
+ * (`rounds` barriers; with `reads` != 0 each round also reads two control
+ * words per CTA, as a near-far iteration does). For tuning the launch
+ * shape. No counterpart in the reference. */
+int mosp_debug_barrier_cost(mosp_workspace *ws, int rounds, int reads,
+                            double *ns_per_round);
 
 #ifdef __cplusplus
 }

@@ -645,6 +645,9 @@ int mosp_workspace_loop_profile(mosp_workspace *ws, int which, unsigned long lon
                                 long long *iters, long long *items) {
   if (ws == nullptr || which < 0 || which > 1) return fail(MOSP_ERR_INVALID, "invalid query");
   const EngineControl &c = ws->hostCtl[which];
+  if (ns) {
+    for (int q = 0; q < 5; ++q) ns[2 + q] = c.iterSplitNs[q];
+  }
   for (int q = 0; q < 2; ++q) {
     if (ns) ns[q] = c.loopNs[q];
     if (iters) iters[q] = c.loopIters[q];
@@ -959,6 +962,21 @@ int mosp_debug_barrier_timeout(mosp_workspace *ws, long long timeout_ms, int *de
                                std::min(ws->shape.engineCtas, 8), s));
   if ((st = readControl(ws, 3, 1, s)) != MOSP_OK) return st;
   if (device_status) *device_status = ws->hostCtl[3].status;
+  return MOSP_OK;
+}
+
+/// Device time of `rounds` grid barriers of the engine's launch shape
+/// (with `reads`, plus the per-iteration control reads); for tuning.
+int mosp_debug_barrier_cost(mosp_workspace *ws, int rounds, int reads, double *ns_per_round) {
+  int st = checkWorkspace(ws);
+  if (st != MOSP_OK) return st;
+  if (rounds <= 0 || rounds > 1000000) return fail(MOSP_ERR_INVALID, "invalid round count");
+  cudaStream_t s = nullptr;
+  MOSP_CUDA(cudaMemsetAsync(ws->ctl + 3, 0, sizeof(EngineControl), s));
+  MOSP_CUDA(launchBarrierCost(ws->ctl + 3, rounds, reads, ws->timeoutNs, ws->shape.engineCtas, s));
+  if ((st = readControl(ws, 3, 1, s)) != MOSP_OK) return st;
+  if (ws->hostCtl[3].status != 0) return fail(MOSP_ERR_TIMEOUT, "barrier cost run timed out");
+  if (ns_per_round) *ns_per_round = static_cast<double>(ws->hostCtl[3].phaseNs[0]) / rounds;
   return MOSP_OK;
 }
 

@@ -210,9 +210,9 @@ enum : int { kDone = 0, kPush = 1, kSplit = 2 };
 constexpr int kStage = 4096;
 
 struct StageHeader {
-  int total;                   // staging attempts (may exceed kStage)
+  int cap;                     // entries per list partition (kStage / (2K))
   int pad;
-  int count[2 * kMaxK];        // staged entries per list (near k, far K+k)
+  int count[2 * kMaxK];        // appends per list this iteration (may exceed cap)
   int base[2 * kMaxK];         // global start of this CTA's range
   u64 farMin[kMaxK];           // minimum distance appended to far (plain)
   long long expanded[kMaxK];   // non-stale expansions (statistics)
@@ -266,7 +266,9 @@ __device__ __forceinline__ Target listTarget(const EngineParams &P, const LoopSh
                 &P.ctl->farMinC[k][s]};
 }
 
-/// Append (v, d) to list l (far lists: d only feeds the pile minimum).
+/// Append (v, d) to list l (far lists: d only feeds the pile minimum). The
+/// staging buffer is split into one partition per list; the rank within the
+/// list is the slot, so a warp group needs one shared atomic.
 __device__ __forceinline__ void stageAppend(const EngineParams &P, const LoopShared &L, int l,
                                             int v, u64 d, int wrSlot, int *nearWV, u64 *nearWD) {
   StageHeader &H = stageHeader();
@@ -276,17 +278,10 @@ __device__ __forceinline__ void stageAppend(const EngineParams &P, const LoopSha
   const unsigned mask = __activemask();
   const unsigned peers = __match_any_sync(mask, l);
   const int leader = __ffs(peers) - 1;
-  int slotBase = 0;
-  if (static_cast<int>(lane) == leader) slotBase = atomicAdd(&H.total, __popc(peers));
-  slotBase = __shfl_sync(peers, slotBase, leader);
-  const int slot = slotBase + __popc(peers & lt);
-  const bool staged = slot < kStage;
-  const unsigned stagedMask = __ballot_sync(peers, staged);
   int rankBase = 0;
-  if (static_cast<int>(lane) == leader && stagedMask != 0) {
-    rankBase = atomicAdd(&H.count[l], __popc(stagedMask));
-  }
+  if (static_cast<int>(lane) == leader) rankBase = atomicAdd(&H.count[l], __popc(peers));
   rankBase = __shfl_sync(peers, rankBase, leader);
+  const int rank = rankBase + __popc(peers & lt);
   if (l >= P.K) {
     // far pile minimum of this CTA (shared), reduced over the group first
     const unsigned hi = static_cast<unsigned>(d >> 32), lo = static_cast<unsigned>(d);
@@ -296,9 +291,10 @@ __device__ __forceinline__ void stageAppend(const EngineParams &P, const LoopSha
       atomicMin(&H.farMin[l - P.K], (static_cast<u64>(mhi) << 32) | mlo);
     }
   }
-  if (staged) {
-    E[slot] = StageEntry{v, (l << 16) | (rankBase + __popc(stagedMask & lt)), d};
+  if (rank < H.cap) {
+    E[l * H.cap + rank] = StageEntry{v, 0, d};
   } else {
+    // partition full: this entry takes the direct global path
     const Target t = listTarget(P, L, l, wrSlot, nearWV, nearWD);
     const int idx = warpAppend(t.counter);
     t.v[idx] = v;
@@ -307,7 +303,8 @@ __device__ __forceinline__ void stageAppend(const EngineParams &P, const LoopSha
 }
 
 /// End of an iteration: reserve every list's range once per CTA, copy the
-/// staged entries out, fold the far minima and the statistics.
+/// staged entries out, fold the far minima. (The expansion counts are
+/// summed per CTA and folded into the statistics after the loop.)
 __device__ void flushStage(const EngineParams &P, const LoopShared &L, int wrSlot, int *nearWV,
                            u64 *nearWD) {
   StageHeader &H = stageHeader();
@@ -315,25 +312,24 @@ __device__ void flushStage(const EngineParams &P, const LoopShared &L, int wrSlo
   const int K = P.K;
   __syncthreads();
   const int t = threadIdx.x;
-  if (t < 2 * K && H.count[t] > 0) {
-    H.base[t] = atomicAdd(listTarget(P, L, t, wrSlot, nearWV, nearWD).counter, H.count[t]);
+  if (t < 2 * K) {
+    const int staged = H.count[t] < H.cap ? H.count[t] : H.cap;
+    if (staged > 0) H.base[t] = atomicAdd(listTarget(P, L, t, wrSlot, nearWV, nearWD).counter, staged);
   }
   if (t < K && H.farMin[t] != kInfWord) {
     atomicMax(listTarget(P, L, K + t, wrSlot, nearWV, nearWD).minC, ~H.farMin[t]);
   }
-  if (t < K && H.expanded[t] != 0) {
-    atomicAdd(reinterpret_cast<unsigned long long *>(&P.ctl->pushes[t]),
-              static_cast<unsigned long long>(H.expanded[t]));
-  }
   __syncthreads();
-  const int total = H.total < kStage ? H.total : kStage;
-  for (int i = t; i < total; i += blockDim.x) {
-    const StageEntry e = E[i];
-    const int l = e.meta >> 16;
+  for (int l = 0; l < 2 * K; ++l) {
+    const int staged = H.count[l] < H.cap ? H.count[l] : H.cap;
+    if (staged == 0) continue;
     const Target tg = listTarget(P, L, l, wrSlot, nearWV, nearWD);
-    const int idx = H.base[l] + (e.meta & 0xffff);
-    tg.v[idx] = e.v;
-    if (tg.d != nullptr) tg.d[idx] = e.d;
+    const int b = H.base[l];
+    for (int i = t; i < staged; i += blockDim.x) {
+      const StageEntry e = E[l * H.cap + i];
+      tg.v[b + i] = e.v;
+      if (tg.d != nullptr) tg.d[b + i] = e.d;
+    }
   }
 }
 
@@ -382,18 +378,18 @@ __device__ bool nearFarLoop(const EngineParams &P, const int *outRow,
     if (deltaOverride != nullptr && lane == 0) delta = *deltaOverride;
   }
 
+  if (threadIdx.x < kMaxK) H.expanded[threadIdx.x] = 0;
   int it = 0;
   unsigned long long profNs[2] = {0, 0};
   long long profIters[2] = {0, 0}, profItems[2] = {0, 0};
+  unsigned long long part[5] = {0, 0, 0, 0, 0};
+  unsigned long long tDecided = 0, tWorked = 0;
   for (;; ++it) {
     const int rdSlot = it % 3, wrSlot = (it + 1) % 3, clrSlot = (it + 2) % 3;
     const unsigned long long itStart = globalNs();
     if (threadIdx.x < 2 * kMaxK) H.count[threadIdx.x] = 0;
-    if (threadIdx.x < kMaxK) {
-      H.farMin[threadIdx.x] = kInfWord;
-      H.expanded[threadIdx.x] = 0;
-    }
-    if (threadIdx.x == 0) H.total = 0;
+    if (threadIdx.x < kMaxK) H.farMin[threadIdx.x] = kInfWord;
+    if (threadIdx.x == 0) H.cap = kStage / (2 * K);
     if (warp == 0) {
       const int k = static_cast<int>(lane);
       const bool act = k < K;
@@ -454,6 +450,7 @@ __device__ bool nearFarLoop(const EngineParams &P, const int *outRow,
     __syncthreads();
     const long long total = L.total;
     if (total == 0) break;
+    if (blockIdx.x == 0 && threadIdx.x == 0) tDecided = globalNs();
 
     const int *nearRV = (it & 1) ? P.nearV1 : P.nearV0;
     const u64 *nearRD = (it & 1) ? P.nearD1 : P.nearD0;
@@ -496,7 +493,20 @@ __device__ bool nearFarLoop(const EngineParams &P, const int *outRow,
           du = tag;
           beg = ldGraph<Mode>(outRow + u);
           deg = ldGraph<Mode>(outRow + u + 1) - beg;
-          atomicAdd(reinterpret_cast<unsigned long long *>(&H.expanded[k]), 1ULL);
+          u = u | 0;  // non-stale
+        } else {
+          u = -1;
+        }
+      }
+      {
+        // statistics: one shared add per objective present in the warp
+        const unsigned live = __ballot_sync(kFull, u >= 0);
+        if (live != 0) {
+          const unsigned peers = __match_any_sync(kFull, u >= 0 ? k : -1);
+          if (u >= 0 && static_cast<int>(lane) == __ffs(peers) - 1) {
+            atomicAdd(reinterpret_cast<unsigned long long *>(&H.expanded[k]),
+                      static_cast<unsigned long long>(__popc(peers)));
+          }
         }
       }
       if (__ballot_sync(kFull, deg > 0) == 0) continue;
@@ -587,17 +597,34 @@ __device__ bool nearFarLoop(const EngineParams &P, const int *outRow,
         }
       }
     }
+    if (blockIdx.x == 0 && threadIdx.x == 0) tWorked = globalNs();
+    __syncthreads();
+    unsigned long long tAll = 0, tFlushed = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) tAll = globalNs();
     flushStage(P, L, wrSlot, nearWV, nearWD);
+    if (blockIdx.x == 0 && threadIdx.x == 0) tFlushed = globalNs();
     if (!gridSync(c, epoch)) return false;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       bool split = false;
       for (int k = 0; k < K; ++k) split |= L.mode[k] == kSplit;
-      profNs[split ? 0 : 1] += globalNs() - itStart;
+      const unsigned long long tEnd = globalNs();
+      profNs[split ? 0 : 1] += tEnd - itStart;
       profIters[split ? 0 : 1] += 1;
       profItems[split ? 0 : 1] += total;
+      if (!split) {
+        part[0] += tDecided - itStart;
+        part[1] += tWorked - tDecided;
+        part[2] += tAll - tWorked;
+        part[3] += tFlushed - tAll;
+        part[4] += tEnd - tFlushed;
+      }
     }
   }
 
+  if (threadIdx.x < K && H.expanded[threadIdx.x] != 0) {
+    atomicAdd(reinterpret_cast<unsigned long long *>(&c->pushes[threadIdx.x]),
+              static_cast<unsigned long long>(H.expanded[threadIdx.x]));
+  }
   if (blockIdx.x == 0 && warp == 0 && static_cast<int>(lane) < K) {
     c->iterations[lane] = iters;
     c->epochs[lane] = epochs;
@@ -609,6 +636,7 @@ __device__ bool nearFarLoop(const EngineParams &P, const int *outRow,
         c->loopIters[q] = profIters[q];
         c->loopItems[q] = profItems[q];
       }
+      for (int q = 0; q < 5; ++q) c->iterSplitNs[q] = part[q];
     }
   }
   return true;
@@ -1350,6 +1378,23 @@ __global__ void barrierProbe(EngineControl *c, long long timeoutNs) {
   gridSync(c, epoch);
 }
 
+/// Cost of the grid barrier alone: `rounds` barriers back to back; with
+/// `reads`, every CTA also reads two control words after each barrier (the
+/// loop's decision step). CTA 0 records the elapsed device time.
+__global__ void barrierCost(EngineControl *c, int rounds, int reads, long long timeoutNs) {
+  Sync epoch = startSync(timeoutNs);
+  const unsigned long long t0 = globalNs();
+  for (int r = 0; r < rounds; ++r) {
+    if (reads && threadIdx.x < 32) {
+      const int a = __ldcg(&c->nearCount[threadIdx.x & 7][r % 3]);
+      const int b = __ldcg(&c->farCount[threadIdx.x & 7][r % 3]);
+      if (a == 12345 && b == 678) c->invalid = 0;
+    }
+    if (!gridSync(c, epoch)) return;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) c->phaseNs[0] = globalNs() - t0;
+}
+
 template <typename Kernel>
 cudaError_t ctasFor(Kernel kernel, int sms, int ctasPerSm, int &ctas, size_t smem = 0) {
   int perSm = 0;
@@ -1408,6 +1453,13 @@ cudaError_t launchBuild(const BuildParams &p, int ctas, cudaStream_t s) {
 cudaError_t launchCosts(const CostParams &p, int ctas, cudaStream_t s) {
   void *args[] = {const_cast<CostParams *>(&p)};
   return cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(pathCosts), dim3(ctas),
+                                     dim3(kThreads), args, 0, s);
+}
+
+cudaError_t launchBarrierCost(EngineControl *ctl, int rounds, int reads, long long timeoutNs,
+                              int ctas, cudaStream_t s) {
+  void *args[] = {&ctl, &rounds, &reads, &timeoutNs};
+  return cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(barrierCost), dim3(ctas),
                                      dim3(kThreads), args, 0, s);
 }
 

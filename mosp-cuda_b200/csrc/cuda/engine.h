@@ -75,6 +75,10 @@ struct alignas(128) EngineControl {
   unsigned long long loopNs[2];
   long long loopIters[2];
   long long loopItems[2];
+  // time (ns) of CTA 0 summed over the push iterations: decision step,
+  // thread 0's own items, waiting for the CTA's other warps, list flush,
+  // grid barrier
+  unsigned long long iterSplitNs[5];
 };
 
 // EngineParams::flags (tuning switches; results do not depend on them)
@@ -156,5 +160,7 @@ cudaError_t launchBuild(const BuildParams &p, int ctas, cudaStream_t s);
 cudaError_t launchCosts(const CostParams &p, int ctas, cudaStream_t s);
 cudaError_t launchBarrierProbe(EngineControl *ctl, long long timeoutNs,
                                int ctas, cudaStream_t s);
+cudaError_t launchBarrierCost(EngineControl *ctl, int rounds, int reads,
+                              long long timeoutNs, int ctas, cudaStream_t s);
 
 }  // namespace mospb200

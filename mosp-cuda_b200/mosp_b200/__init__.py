@@ -86,6 +86,7 @@ _SIGS = {
     "mosp_update_host": (_i, [_p, _i, _i, _i, _p, _p, _p, _i, _p, _p, _p, _i, _p, _p, _p, _p, _i,
                               _i, _ip, _ll, _p, _p, _p, _p, _p, C.POINTER(Timings)]),
     "mosp_debug_barrier_timeout": (_i, [_p, _ll, _ip]),
+    "mosp_debug_barrier_cost": (_i, [_p, _i, _i, C.POINTER(C.c_double)]),
     # host side
     "mosp_graph_read": (_i, [C.c_char_p, C.c_char_p, C.POINTER(_p)]),
     "mosp_graph_write": (_i, [_p, C.c_char_p]),
@@ -401,11 +402,14 @@ class Workspace:
     def loop_profile(self, which=0):
         """Near-far loop of the last launch: {split|push: (ms, iterations,
         items)}."""
-        ns = (C.c_ulonglong * 2)()
+        ns = (C.c_ulonglong * 7)()
         it = (C.c_longlong * 2)()
         items = (C.c_longlong * 2)()
         check(lib().mosp_workspace_loop_profile(self._h, which, ns, it, items))
-        return {name: (round(ns[q] / 1e6, 4), it[q], items[q]) for q, name in enumerate(("split", "push"))}
+        out = {name: (round(ns[q] / 1e6, 4), it[q], items[q]) for q, name in enumerate(("split", "push"))}
+        out["push_parts_ms"] = {name: round(ns[2 + q] / 1e6, 4) for q, name in
+                                enumerate(("decide", "own_items", "wait_cta", "flush", "barrier"))}
+        return out
 
     def grid(self) -> int:
         c = C.c_int()
@@ -498,6 +502,11 @@ class Workspace:
                                      _ptr(init_dist), _ptr(init_parent), K, source, pa, int(delta),
                                      _ptr(dist), _ptr(par), _ptr(cd), _ptr(cp), _ptr(cost), C.byref(t)))
         return dist.reshape(K, n), par.reshape(K, n), cd, cp, (cost.reshape(n, KG) if costs else None), t
+
+    def barrier_cost_ns(self, rounds=2000, reads=False) -> float:
+        x = C.c_double()
+        check(lib().mosp_debug_barrier_cost(self._h, rounds, int(reads), C.byref(x)))
+        return x.value
 
     def barrier_timeout_probe(self, timeout_ms: int) -> int:
         st = C.c_int(-1)
