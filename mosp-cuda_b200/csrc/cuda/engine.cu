@@ -486,17 +486,14 @@ __device__ bool nearFarLoop(const EngineParams &P, const int *outRow,
       u64 du = 0;
       if (mode == kPush) {
         const long long kn = static_cast<long long>(k) * P.strideNear;
+        // A stale entry (the word has dropped below its tag since) is
+        // expanded with its tag: its offers are strictly larger than the
+        // ones of the newer entry, so they never win a word. Skipping the
+        // check saves a dependent load on every expansion.
         u = __ldcg(nearRV + kn + i);
-        const u64 tag = __ldcg(nearRD + kn + i);
-        const u64 word = __ldcg(P.packed + ko + u);
-        if (word != kInfWord && pkOf(P.obj[k]).dist(word) == tag) {
-          du = tag;
-          beg = ldGraph<Mode>(outRow + u);
-          deg = ldGraph<Mode>(outRow + u + 1) - beg;
-          u = u | 0;  // non-stale
-        } else {
-          u = -1;
-        }
+        du = __ldcg(nearRD + kn + i);
+        beg = ldGraph<Mode>(outRow + u);
+        deg = ldGraph<Mode>(outRow + u + 1) - beg;
       }
       {
         // statistics: one shared add per objective present in the warp
@@ -844,8 +841,6 @@ __global__ void __launch_bounds__(kThreads, 1) sospEngine(const __grid_constant_
   const long long T = static_cast<long long>(gridDim.x) * blockDim.x;
   const unsigned lane = laneId();
   const int warp = threadIdx.x >> 5;
-  const long long gwarp = tid >> 5;
-  const long long nwarps = T >> 5;
   Sync epoch = startSync(P.timeoutNs);
   // Stamp generations of this launch start after the previous launch's.
   const int genBase = __ldcg(P.genPtr) + 1;
@@ -946,19 +941,42 @@ __global__ void __launch_bounds__(kThreads, 1) sospEngine(const __grid_constant_
 
     markPhase(c, kPhaseJumped);
     // ---- Invalidate; candidates = invalidated + insert heads (:293-313) ---
+    // Each CTA compacts its contiguous vertex range with block scans and
+    // reserves its part of the candidate list with one atomic per objective.
+    {
+      __shared__ int sBase;
+      const long long chunk = (static_cast<long long>(n) + gridDim.x - 1) / gridDim.x;
+      const long long lo = static_cast<long long>(blockIdx.x) * chunk < n
+                               ? static_cast<long long>(blockIdx.x) * chunk : n;
+      const long long hi = lo + chunk < n ? lo + chunk : n;
+      for (int k = 0; k < K; ++k) {
+        const long long ko = static_cast<long long>(k) * P.stride;
+        long long cnt = 0;
+        for (long long v = lo + threadIdx.x; v < hi; v += blockDim.x) {
+          cnt += __ldcg(P.val + ko + v) == -2 ? 1 : 0;
+        }
+        const long long found = blockSum(cnt);
+        if (threadIdx.x == 0) {
+          sBase = found > 0 ? atomicAdd(&c->candCount[k], static_cast<int>(found)) : 0;
+          if (found > 0) atomicAdd(&c->invalidated[k], static_cast<int>(found));
+        }
+        __syncthreads();
+        long long carry = sBase;
+        for (long long t0 = lo; t0 < hi; t0 += blockDim.x) {
+          const long long v = t0 + threadIdx.x;
+          const bool inv = v < hi && __ldcg(P.val + ko + v) == -2;
+          long long tileTotal;
+          const long long incl = blockInclusiveScan(inv ? 1 : 0, &tileTotal);
+          if (inv) {
+            P.packed[ko + v] = kInfWord;
+            P.cand[ko + carry + incl - 1] = static_cast<int>(v);
+          }
+          carry += tileTotal;
+        }
+      }
+    }
     for (int k = 0; k < K; ++k) {
       const long long ko = static_cast<long long>(k) * P.stride;
-      for (long long base = gwarp * 32; base < n; base += nwarps * 32) {
-        const long long v = base + lane;
-        const bool inv = v < n && __ldcg(P.val + ko + v) == -2;
-        const unsigned ballot = __ballot_sync(kFull, inv);
-        if (inv) {
-          P.packed[ko + v] = kInfWord;
-          const int idx = warpAppend(&c->candCount[k]);
-          P.cand[ko + idx] = static_cast<int>(v);
-        }
-        if (lane == 0 && ballot != 0) atomicAdd(&c->invalidated[k], __popc(ballot));
-      }
       for (long long i = tid; i < P.nHeads; i += T) {
         const int v = P.heads[i];
         if (v < 0 || v >= n) {
@@ -992,10 +1010,46 @@ __global__ void __launch_bounds__(kThreads, 1) sospEngine(const __grid_constant_
         sOff[lane] = incl - cnt;
         if (lane == 31) sOff[kMaxK] = incl;
       }
+      StageHeader &H = stageHeader();
+      StageEntry *E = stageEntries();
+      if (threadIdx.x < kMaxK) {
+        H.count[threadIdx.x] = 0;
+        H.farMin[threadIdx.x] = kInfWord;
+      }
+      if (threadIdx.x == 0) H.cap = kStage / K;
       __syncthreads();
       const long long total = sOff[kMaxK];
-      for (long long base = gwarp * 32; base < total; base += nwarps * 32) {
-        const long long j = base + lane;
+      // Improved candidates go to far pile 0. With a partition of at least
+      // one tile per objective (K * blockDim <= kStage) the appends are
+      // staged per CTA and written out with one reservation per objective
+      // when a partition could fill up and at the end; otherwise each warp
+      // appends to the global pile directly.
+      const bool staged = K * static_cast<int>(blockDim.x) <= kStage;
+      auto flushPull = [&]() {
+        __syncthreads();
+        if (threadIdx.x < K && H.count[threadIdx.x] > 0) {
+          H.base[threadIdx.x] = atomicAdd(&c->farCount[threadIdx.x][0], H.count[threadIdx.x]);
+          atomicMax(&c->farMinC[threadIdx.x][0], ~H.farMin[threadIdx.x]);
+        }
+        __syncthreads();
+        for (int k = 0; k < K; ++k) {
+          const int cnt = H.count[k];
+          const long long ko = static_cast<long long>(k) * P.stride;
+          for (int q = threadIdx.x; q < cnt; q += blockDim.x) {
+            P.farL0[ko + H.base[k] + q] = E[k * H.cap + q].v;
+          }
+        }
+        __syncthreads();
+        if (threadIdx.x < kMaxK) {
+          H.count[threadIdx.x] = 0;
+          H.farMin[threadIdx.x] = kInfWord;
+        }
+        __syncthreads();
+      };
+      const long long tileStride = static_cast<long long>(gridDim.x) * blockDim.x;
+      for (long long tile = static_cast<long long>(blockIdx.x) * blockDim.x; tile < total;
+           tile += tileStride) {
+        const long long j = tile + threadIdx.x;
         const bool valid = j < total;
         int k = 0;
         if (valid) {
@@ -1055,12 +1109,37 @@ __global__ void __launch_bounds__(kThreads, 1) sospEngine(const __grid_constant_
           P.packed[ko + v] = best;
           if (pk.dist(best) < (cur == kInfWord ? kInfWord : pk.dist(cur))) {
             P.inFar[ko + v] = 1;
-            const int idx = warpAppend(&c->farCount[k][0]);
-            P.farL0[ko + idx] = v;
-            warpMinInto(&c->farMinC[k][0], pk.dist(best));
+            if (!staged) {
+              const int idx = warpAppend(&c->farCount[k][0]);
+              P.farL0[ko + idx] = v;
+              warpMinInto(&c->farMinC[k][0], pk.dist(best));
+              continue;
+            }
+            const unsigned peers = __match_any_sync(__activemask(), k);
+            const int leader = __ffs(peers) - 1;
+            int rb = 0;
+            if (static_cast<int>(lane) == leader) rb = atomicAdd(&H.count[k], __popc(peers));
+            rb = __shfl_sync(peers, rb, leader);
+            E[k * H.cap + rb + __popc(peers & ((1u << lane) - 1u))].v = v;
+            const u64 d = pk.dist(best);
+            const unsigned hi = static_cast<unsigned>(d >> 32), lo = static_cast<unsigned>(d);
+            const unsigned mhi = __reduce_min_sync(peers, hi);
+            const unsigned mlo = __reduce_min_sync(peers, hi == mhi ? lo : 0xffffffffu);
+            if (static_cast<int>(lane) == leader) {
+              atomicMin(&H.farMin[k], (static_cast<u64>(mhi) << 32) | mlo);
+            }
           }
         }
+        if (!staged) continue;
+        // a tile appends at most blockDim entries: flush before a partition
+        // could overflow
+        __syncthreads();
+        if (__syncthreads_or(threadIdx.x < static_cast<unsigned>(K) &&
+                             H.count[threadIdx.x] > H.cap - static_cast<int>(blockDim.x))) {
+          flushPull();
+        }
       }
+      if (staged) flushPull();
     }
     if (!gridSync(c, epoch)) return;
     markPhase(c, kPhasePulled);
