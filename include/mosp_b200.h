@@ -236,6 +236,37 @@ int mosp_sosp_from_scratch(mosp_workspace *ws, int n, int m,
                            int *d_parent, mosp_sosp_stats *stats,
                            void *stream);
 
+/* Limits of mosp_sosp_from_scratch_static: its scratch is a fixed device
+ * array of about 10 MB sized for these. */
+#define MOSP_STATIC_MAX_VERTICES 65536
+#define MOSP_STATIC_MAX_EDGES 262144
+
+/* mosp_sosp_from_scratch without a workspace and without any device or
+ * pinned allocation, for callers that cannot allocate during a call (device
+ * memory owned by another allocator or a fixed budget; latency-critical
+ * handlers, where an allocation may synchronize the device; plugin hosts
+ * that forbid it). The engine's scratch is a file-scope __device__ array
+ * reserved when the library's module is loaded, one per device; results
+ * equal mosp_sosp_from_scratch's. No counterpart in the reference (whose
+ * sospFromScratchGpu allocates, src/sospUpdateGpu.cu:719-745).
+ *   - n <= MOSP_STATIC_MAX_VERTICES and m <= MOSP_STATIC_MAX_EDGES; larger
+ *     graphs are rejected with MOSP_ERR_INVALID and a message.
+ *   - Runs on the current device. The first call on a device does the
+ *     setup (module load, symbol address, launch-shape query); make it
+ *     before any stream capture on that device.
+ *   - The call clears the scratch regions that must start at zero (control
+ *     block, stamp generation, stamps, in-far flags) in `stream` before the
+ *     launch, so an aborted call leaves nothing behind.
+ *   - Calls on one device share the scratch: calls that overlap in time
+ *     (two host threads, or unordered streams) race and must be serialized
+ *     by the caller. A call returns after its result is complete. */
+int mosp_sosp_from_scratch_static(int n, int m, const int *d_out_row,
+                                  const int *d_out_col, const int *d_out_w,
+                                  int source, long long delta,
+                                  long long max_weight, long long *d_dist,
+                                  int *d_parent, mosp_sosp_stats *stats,
+                                  void *stream);
+
 /* Steps 2-3 of the MOSP update in one persistent launch: build the
  * combined graph of the K trees d_parents[k*n+v] (edge (p,v) iff p is the
  * parent of v in some tree; weight L*(K+1) - sum_{i: Parent_i[v]==p}

@@ -42,6 +42,8 @@ constexpr int kControlBlocks = 4;  // 0: update/scratch, 1: combined, 2: build, 
 
 }  // namespace
 
+int mospb200::recordFailure(int status, const char *message) { return fail(status, message); }
+
 // ---------------------------------------------------------------------------
 // Workspace
 // ---------------------------------------------------------------------------

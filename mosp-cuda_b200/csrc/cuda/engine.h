@@ -163,4 +163,8 @@ cudaError_t launchBarrierProbe(EngineControl *ctl, long long timeoutNs,
 cudaError_t launchBarrierCost(EngineControl *ctl, int rounds, int reads,
                               long long timeoutNs, int ctas, cudaStream_t s);
 
+/// Sets the calling thread's last-error message of the C ABI
+/// (mosp_last_error) and returns `status`.
+int recordFailure(int status, const char *message);
+
 }  // namespace mospb200

@@ -78,6 +78,8 @@ _SIGS = {
                                     C.POINTER(_p), C.POINTER(_p), C.POINTER(SospStats), _p]),
     "mosp_sosp_from_scratch": (_i, [_p, _i, _i, _p, _p, _p, _i, _ll, _ll, _p, _p,
                                     C.POINTER(SospStats), _p]),
+    "mosp_sosp_from_scratch_static": (_i, [_i, _i, _p, _p, _p, _i, _ll, _ll, _p, _p,
+                                           C.POINTER(SospStats), _p]),
     "mosp_combined_sosp": (_i, [_p, _i, _i, _p, _ip, _i, _ll, _p, _p, C.POINTER(CombineStats), _p]),
     "mosp_path_costs": (_i, [_p, _i, _i, _i, _p, _p, _p, _p, _i, _p, _p]),
     "mosp_update_device": (_i, [_p, _i, _i, _i, _p, _p, _p, _p, _p, _p, _p, _p, _ip, _p, _i, _i,
