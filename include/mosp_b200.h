@@ -226,6 +226,29 @@ int mosp_sosp_update_multi(
     long long *const *h_dist, int *const *h_parent, mosp_sosp_stats *stats,
     void *stream);
 
+/* Step 1 on the GPU: applies a change batch to a device out-CSR (edge-major
+ * weights w[e*K+k], as in the reference's host CsrGraph) and writes the
+ * updated out-CSR, which needs room for m + n_ins edges (new_capacity), and
+ * the weight-increase mask of every insertion. *new_m receives the updated
+ * edge count. Deletions come first (each removes the first live (u,v) in
+ * its row, in file order), then insertions (each overwrites the first live
+ * (u,v) or appends at the end of its row); the result equals the host
+ * applyChangeBatch edge for edge. When h_max_weight / h_weight_sum are
+ * non-NULL they receive (K entries each) the largest weight of the original
+ * edges and insertions (at least 1) and the weight sum of the original
+ * edges, the inputs of the default delta. Replaces applyChangeBatch
+ * (src/csrGraph.cu:727-894) and the per-objective statistics of mospUpdate
+ * (src/mospUpdate.cu:104-136). */
+int mosp_apply_batch_device(mosp_workspace *ws, int n, int K, int m,
+                            const int *d_row, const int *d_col, const int *d_w,
+                            int n_ins, const int *d_ins_from,
+                            const int *d_ins_to, const int *d_ins_w, int n_del,
+                            const int *d_del_from, const int *d_del_to,
+                            int *d_new_row, int *d_new_col, int *d_new_w,
+                            long long new_capacity, int *new_m,
+                            unsigned *d_mask, long long *h_max_weight,
+                            long long *h_weight_sum, void *stream);
+
 /* Canonical single-source shortest paths from scratch. Replaces
  * sospFromScratchGpu (headers/sospUpdateGpu.cuh:107-110,
  * src/sospUpdateGpu.cu:719-745). */

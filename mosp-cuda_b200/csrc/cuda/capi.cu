@@ -89,6 +89,9 @@ struct mosp_workspace {
   // caller buffers (mosp_workspace_buffer)
   void *user[32] = {nullptr};
   unsigned long long userBytes[32] = {0};
+  // Step 1 scratch (mosp_apply_batch_device)
+  void *applyScratch = nullptr;
+  size_t applyBytes = 0;
 };
 
 namespace {
@@ -574,6 +577,7 @@ void mosp_workspace_destroy(mosp_workspace *ws) {
   for (void *p : ws->user) {
     if (p) cudaFree(p);
   }
+  if (ws->applyScratch) cudaFree(ws->applyScratch);
   for (cudaEvent_t e : ws->ev) {
     if (e) cudaEventDestroy(e);
   }
@@ -704,6 +708,73 @@ int mosp_build_device_graph(mosp_workspace *ws, int n, int m, int K, const int *
     return fail(MOSP_ERR_INVALID,
                 "Error: malformed CSR (row offsets not monotone from 0 to m, or a column index "
                 "outside [0, n)).");
+  }
+  return MOSP_OK;
+}
+
+int mosp_apply_batch_device(mosp_workspace *ws, int n, int K, int m, const int *d_row,
+                            const int *d_col, const int *d_w, int n_ins, const int *d_ins_from,
+                            const int *d_ins_to, const int *d_ins_w, int n_del,
+                            const int *d_del_from, const int *d_del_to, int *d_new_row,
+                            int *d_new_col, int *d_new_w, long long new_capacity, int *new_m,
+                            unsigned *d_mask, long long *h_max_weight, long long *h_weight_sum,
+                            void *stream) {
+  int st = checkWorkspace(ws);
+  if (st != MOSP_OK) return st;
+  if (n <= 0 || K < 1 || K > kMaxK || m < 0 || n_ins < 0 || n_del < 0 || d_row == nullptr ||
+      (m > 0 && (d_col == nullptr || d_w == nullptr)) ||
+      (n_ins > 0 && (d_ins_from == nullptr || d_ins_to == nullptr || d_ins_w == nullptr ||
+                     d_mask == nullptr)) ||
+      (n_del > 0 && (d_del_from == nullptr || d_del_to == nullptr)) || d_new_row == nullptr ||
+      d_new_col == nullptr || d_new_w == nullptr || new_m == nullptr ||
+      new_capacity < static_cast<long long>(m) + n_ins ||
+      static_cast<long long>(m) + n_ins > INT_MAX) {
+    return fail(MOSP_ERR_INVALID, "Error: invalid change-batch arguments (the updated graph needs "
+                                  "room for m + n_ins edges).");
+  }
+  const size_t need = applyScratchBytes(n, m, n_ins, n_del);
+  if (need > ws->applyBytes) {
+    if (ws->applyScratch) cudaFree(ws->applyScratch);
+    ws->applyScratch = nullptr;
+    ws->applyBytes = 0;
+    unsigned char *p = nullptr;
+    if ((st = deviceAlloc(&p, need)) != MOSP_OK) return st;
+    ws->applyScratch = p;
+    ws->applyBytes = need;
+  }
+  int sms = 0;
+  MOSP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ws->device));
+  ApplyParams P;
+  std::memset(&P, 0, sizeof(P));
+  P.n = n;
+  P.m = m;
+  P.K = K;
+  P.row = d_row;
+  P.col = d_col;
+  P.w = d_w;
+  P.nIns = n_ins;
+  P.nDel = n_del;
+  P.insFrom = d_ins_from;
+  P.insTo = d_ins_to;
+  P.insW = d_ins_w;
+  P.delFrom = d_del_from;
+  P.delTo = d_del_to;
+  P.newRow = d_new_row;
+  P.newCol = d_new_col;
+  P.newW = d_new_w;
+  P.mask = d_mask;
+  int counters[kApplyCounters + 1] = {0};
+  long long stats[2 * kMaxK] = {0};
+  const bool wantStats = h_max_weight != nullptr || h_weight_sum != nullptr;
+  MOSP_CUDA(applyBatchGpu(P, ws->applyScratch, sms, asStream(stream), counters,
+                          wantStats ? stats : nullptr));
+  if (counters[kApplyInvalid]) {
+    return fail(MOSP_ERR_INVALID, "Error: a changed edge's endpoint is out of range.");
+  }
+  *new_m = counters[kApplyCounters];
+  for (int k = 0; k < K && wantStats; ++k) {
+    if (h_max_weight) h_max_weight[k] = stats[k];
+    if (h_weight_sum) h_weight_sum[k] = stats[K + k];
   }
   return MOSP_OK;
 }

@@ -163,6 +163,52 @@ cudaError_t launchBarrierProbe(EngineControl *ctl, long long timeoutNs,
 cudaError_t launchBarrierCost(EngineControl *ctl, int rounds, int reads,
                               long long timeoutNs, int ctas, cudaStream_t s);
 
+// ---------------------------------------------------------------------------
+// Step 1 on the GPU (apply.cu): a change batch applied to a device CSR
+// ---------------------------------------------------------------------------
+struct ApplyParams {
+  long long n, m;
+  int K;
+  const int *row, *col, *w;  // original out-CSR, edge-major weights w[e*K+k]
+  int nIns, nDel;
+  const int *insFrom, *insTo, *insW, *delFrom, *delTo;
+  int *newRow, *newCol, *newW;  // updated out-CSR (capacity m + nIns edges)
+  unsigned *mask;               // nIns weight-increase masks
+  // set by applyBatchGpu
+  int vbits, ibits;
+  const int *sortedVals;
+};
+
+/// Per (u,v) group of the sorted batch.
+struct ApplyGroups {
+  int *start;  // first entry of each group (+ end sentinel)
+  int *u, *v, *cD, *cI, *firstIns, *lastIns, *occ, *first;
+};
+
+/// Rows with at least one change.
+struct ApplyRows {
+  int *row, *gs, *deg, *off;
+};
+
+enum ApplyCounter : int {
+  kApplyInvalid = 0,
+  kApplyEntries,
+  kApplyGroups,
+  kApplyRows,
+  kApplyAppended,
+  kApplyCounters
+};
+
+/// Scratch bytes of applyBatchGpu for these sizes.
+size_t applyScratchBytes(long long n, long long m, long long nIns, long long nDel);
+/// Runs Step 1 on stream `s` and waits for it. hostCounters receives the
+/// kApplyCounters device counters followed by the new edge count; when
+/// hostStats is non-null it receives per objective the largest weight of
+/// the original edges and insertions (at least 1), then the weight sums of
+/// the original edges (2K values).
+cudaError_t applyBatchGpu(ApplyParams P, void *scratch, int sms, cudaStream_t s, int *hostCounters,
+                          long long *hostStats);
+
 /// Sets the calling thread's last-error message of the C ABI
 /// (mosp_last_error) and returns `status`.
 int recordFailure(int status, const char *message);

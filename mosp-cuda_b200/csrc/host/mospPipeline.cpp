@@ -1,10 +1,10 @@
 // mospPipeline.cpp - one MOSP update from host memory (the reference's
 // in-memory pipeline, SMShovan/MOSP-CUDA src/mospUpdate.cu:57-225) and the
 // file-based wrappers (src/parallelSOSPUpdate.cu, src/parallelCombinedGraph
-// .cu). Stages: apply the batch on the host, upload the updated out-CSR
-// once (the reverse CSR and weight columns are built on the GPU), run the
-// K SOSP updates as one fused launch and Steps 2-3 as a second one,
-// optionally the MOSP path costs on the GPU, download.
+// .cu). Stages: upload the original out-CSR, the batch and the trees; apply
+// the batch on the GPU (Step 1), build the reverse CSR and weight columns on
+// the GPU, run the K SOSP updates as one fused launch and Steps 2-3 as a
+// second one, optionally the MOSP path costs on the GPU, download.
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
@@ -37,7 +37,8 @@ double msSince(std::chrono::steady_clock::time_point t) {
 /// repeated runs reuse them.
 enum Slot : int {
   kOutRow, kOutCol, kEdgeW, kOutW, kInRow, kInCol, kInW, kDist, kParent, kHeads,
-  kChFrom, kChTo, kCombDist, kCombParent, kCosts
+  kChFrom, kChTo, kCombDist, kCombParent, kCosts, kOrigRow, kOrigCol, kOrigW, kInsFrom,
+  kInsW, kDelFrom, kDelTo, kMask
 };
 
 template <typename T>
@@ -85,6 +86,7 @@ struct PipelineIn {
   const int *pref = nullptr;            // K values or null
   long long delta = 0;
   bool costs = false;
+  bool wantUpdated = false;  // download the updated graph into PipelineOut::updated
 };
 
 struct PipelineOut {
@@ -120,40 +122,77 @@ int runPipeline(mosp_workspace *ws, const PipelineIn &in, PipelineOut &out, std:
       return MOSP_ERR_INVALID;
     }
   }
-  // --- apply the batch (host) -------------------------------------------------
+  if (in.b.K != KG) {
+    err = "Error: change batch has " + std::to_string(in.b.K) + " objectives, graph has " +
+          std::to_string(KG) + ".";
+    return MOSP_ERR_INVALID;
+  }
+  const long long m0 = in.g.edges();
+  const int nIns = in.b.nIns, nDel = in.b.nDel;
+  const size_t kn = static_cast<size_t>(K) * n;
+  const size_t cap = static_cast<size_t>(m0) + nIns;
+
+  // --- upload the original graph, the batch and the trees -----------------------
   auto t0 = std::chrono::steady_clock::now();
+  int *dOrigRow, *dOrigCol, *dOrigW, *dInsFrom, *dInsTo, *dInsW, *dDelFrom, *dDelTo;
+  unsigned *dMask;
+  int *dOutRow, *dOutCol, *dEdgeW, *dOutW, *dInRow, *dInCol, *dInW, *dParent, *dChFrom, *dChTo,
+      *dCombParent;
+  long long *dDist, *dCombDist, *dCosts = nullptr;
   {
-    ScopedStage stage("apply_batch_host");
-    if (!applyBatchView(in.g, in.b, out.updated, out.mask)) {
-      err = "Error: the change batch does not match the graph.";
-      return MOSP_ERR_INVALID;
+    ScopedStage stage("upload", true);
+    if (!slot(ws, kOrigRow, static_cast<size_t>(n) + 1, dOrigRow, err) ||
+        !slot(ws, kOrigCol, m0, dOrigCol, err) ||
+        !slot(ws, kOrigW, static_cast<size_t>(m0) * KG, dOrigW, err) ||
+        !slot(ws, kInsFrom, nIns, dInsFrom, err) || !slot(ws, kHeads, nIns, dInsTo, err) ||
+        !slot(ws, kInsW, static_cast<size_t>(nIns) * KG, dInsW, err) ||
+        !slot(ws, kDelFrom, nDel, dDelFrom, err) || !slot(ws, kDelTo, nDel, dDelTo, err) ||
+        !slot(ws, kMask, nIns, dMask, err) || !slot(ws, kDist, kn, dDist, err) ||
+        !slot(ws, kParent, kn, dParent, err)) {
+      return MOSP_ERR_OOM;
+    }
+    if (!toDevice(dOrigRow, in.g.row, static_cast<size_t>(n) + 1, err) ||
+        !toDevice(dOrigCol, in.g.col, m0, err) ||
+        !toDevice(dOrigW, in.g.w, static_cast<size_t>(m0) * KG, err) ||
+        !toDevice(dInsFrom, in.b.insFrom, nIns, err) || !toDevice(dInsTo, in.b.insTo, nIns, err) ||
+        !toDevice(dInsW, in.b.insW, static_cast<size_t>(nIns) * KG, err) ||
+        !toDevice(dDelFrom, in.b.delFrom, nDel, err) || !toDevice(dDelTo, in.b.delTo, nDel, err) ||
+        !toDevice(dDist, in.initDist, kn, err) || !toDevice(dParent, in.initParent, kn, err)) {
+      return MOSP_ERR_CUDA;
     }
   }
-  out.t.apply_batch = msSince(t0);
-  const CsrGraph &up = out.updated;
-  const long long m0 = in.g.edges();
-  const int m = up.numberOfEdges();
+  out.t.upload = msSince(t0);
 
+  // --- Step 1 on the GPU: apply the batch ------------------------------------------
   // per objective: largest weight (original edges and inserts), weight sum
   // of the original edges, and the changes that may invalidate a subtree
-  std::vector<long long> maxWeight(K, 1), weightSum(K, 0), delta(K, in.delta);
-  for (long long e = 0; e < m0; ++e) {
-    for (int k = 0; k < K; ++k) {
-      const int w = in.g.weight(e, k);
-      maxWeight[k] = std::max(maxWeight[k], static_cast<long long>(w));
-      weightSum[k] += w;
+  t0 = std::chrono::steady_clock::now();
+  std::vector<long long> maxWeight(KG, 1), weightSum(KG, 0), delta(K, in.delta);
+  int m = 0;
+  {
+    ScopedStage stage("apply_batch_gpu", true);
+    if (!slot(ws, kOutRow, static_cast<size_t>(n) + 1, dOutRow, err) ||
+        !slot(ws, kOutCol, cap, dOutCol, err) || !slot(ws, kEdgeW, cap * KG, dEdgeW, err)) {
+      return MOSP_ERR_OOM;
     }
-  }
-  for (int i = 0; i < in.b.nIns; ++i) {
-    for (int k = 0; k < K; ++k) {
-      maxWeight[k] = std::max(maxWeight[k], static_cast<long long>(in.b.insW[static_cast<size_t>(i) * KG + k]));
+    int st = mosp_apply_batch_device(ws, n, KG, static_cast<int>(m0), dOrigRow, dOrigCol, dOrigW,
+                                     nIns, dInsFrom, dInsTo, dInsW, nDel, dDelFrom, dDelTo,
+                                     dOutRow, dOutCol, dEdgeW, static_cast<long long>(cap), &m,
+                                     dMask, maxWeight.data(), weightSum.data(), nullptr);
+    if (st != MOSP_OK) {
+      err = mosp_last_error();
+      return st;
+    }
+    out.mask.assign(nIns, 0u);
+    if (!toHost(out.mask.data(), dMask, nIns, err)) {
+      return MOSP_ERR_CUDA;
     }
   }
   std::vector<int> chFrom, chTo, chOffset(K + 1, 0);
   for (int k = 0; k < K; ++k) {
-    chFrom.insert(chFrom.end(), in.b.delFrom, in.b.delFrom + in.b.nDel);
-    chTo.insert(chTo.end(), in.b.delTo, in.b.delTo + in.b.nDel);
-    for (int i = 0; i < in.b.nIns; ++i) {
+    chFrom.insert(chFrom.end(), in.b.delFrom, in.b.delFrom + nDel);
+    chTo.insert(chTo.end(), in.b.delTo, in.b.delTo + nDel);
+    for (int i = 0; i < nIns; ++i) {
       if (out.mask[i] & (1u << k)) {
         chFrom.push_back(in.b.insFrom[i]);
         chTo.push_back(in.b.insTo[i]);
@@ -164,37 +203,40 @@ int runPipeline(mosp_workspace *ws, const PipelineIn &in, PipelineOut &out, std:
       delta[k] = mosp_default_delta(m0 > 0 ? m0 : std::max(m, 1), n, weightSum[k]);
     }
   }
+  if (!slot(ws, kChFrom, chFrom.size(), dChFrom, err) ||
+      !slot(ws, kChTo, chTo.size(), dChTo, err) ||
+      !toDevice(dChFrom, chFrom.data(), chFrom.size(), err) ||
+      !toDevice(dChTo, chTo.data(), chTo.size(), err)) {
+    return MOSP_ERR_CUDA;
+  }
+  if (in.wantUpdated) {
+    // the reference API returns the updated graph on the host
+    CsrGraph &up = out.updated;
+    up = CsrGraph();
+    up.numberOfNodes = n;
+    up.numberOfObjectives = KG;
+    up.rowPtr.resize(static_cast<size_t>(n) + 1);
+    up.colInd.resize(m);
+    up.weights.resize(static_cast<size_t>(m) * KG);
+    if (!toHost(up.rowPtr.data(), dOutRow, up.rowPtr.size(), err) ||
+        !toHost(up.colInd.data(), dOutCol, up.colInd.size(), err) ||
+        !toHost(up.weights.data(), dEdgeW, up.weights.size(), err)) {
+      return MOSP_ERR_CUDA;
+    }
+  }
+  out.t.apply_batch = msSince(t0);
 
-  // --- upload -------------------------------------------------------------------
+  // --- device graph: weight columns and reverse CSR, built on the GPU --------------
   t0 = std::chrono::steady_clock::now();
-  int *dOutRow, *dOutCol, *dEdgeW, *dOutW, *dInRow, *dInCol, *dInW, *dParent, *dHeads, *dChFrom,
-      *dChTo, *dCombParent;
-  long long *dDist, *dCombDist, *dCosts = nullptr;
-  const size_t kn = static_cast<size_t>(K) * n;
   {
-    ScopedStage stage("upload", true);
-    if (!slot(ws, kOutRow, static_cast<size_t>(n) + 1, dOutRow, err) ||
-        !slot(ws, kOutCol, m, dOutCol, err) ||
-        !slot(ws, kEdgeW, static_cast<size_t>(m) * KG, dEdgeW, err) ||
-        !slot(ws, kOutW, static_cast<size_t>(m) * KG, dOutW, err) ||
+    ScopedStage stage("build_device_graph", true);
+    if (!slot(ws, kOutW, static_cast<size_t>(m) * KG, dOutW, err) ||
         !slot(ws, kInRow, static_cast<size_t>(n) + 1, dInRow, err) ||
         !slot(ws, kInCol, m, dInCol, err) ||
-        !slot(ws, kInW, static_cast<size_t>(m) * KG, dInW, err) || !slot(ws, kDist, kn, dDist, err) ||
-        !slot(ws, kParent, kn, dParent, err) || !slot(ws, kHeads, in.b.nIns, dHeads, err) ||
-        !slot(ws, kChFrom, chFrom.size(), dChFrom, err) ||
-        !slot(ws, kChTo, chTo.size(), dChTo, err) || !slot(ws, kCombDist, n, dCombDist, err) ||
-        !slot(ws, kCombParent, n, dCombParent, err) ||
+        !slot(ws, kInW, static_cast<size_t>(m) * KG, dInW, err) ||
+        !slot(ws, kCombDist, n, dCombDist, err) || !slot(ws, kCombParent, n, dCombParent, err) ||
         (in.costs && !slot(ws, kCosts, static_cast<size_t>(n) * KG, dCosts, err))) {
       return MOSP_ERR_OOM;
-    }
-    if (!toDevice(dOutRow, up.rowPtr.data(), up.rowPtr.size(), err) ||
-        !toDevice(dOutCol, up.colInd.data(), up.colInd.size(), err) ||
-        !toDevice(dEdgeW, up.weights.data(), up.weights.size(), err) ||
-        !toDevice(dDist, in.initDist, kn, err) || !toDevice(dParent, in.initParent, kn, err) ||
-        !toDevice(dHeads, in.b.insTo, static_cast<size_t>(in.b.nIns), err) ||
-        !toDevice(dChFrom, chFrom.data(), chFrom.size(), err) ||
-        !toDevice(dChTo, chTo.data(), chTo.size(), err)) {
-      return MOSP_ERR_CUDA;
     }
     const int st = mosp_build_device_graph(ws, n, m, KG, dOutRow, dOutCol, dEdgeW, dOutW, dInRow,
                                            dInCol, dInW, nullptr);
@@ -203,7 +245,7 @@ int runPipeline(mosp_workspace *ws, const PipelineIn &in, PipelineOut &out, std:
       return st;
     }
   }
-  out.t.upload = msSince(t0);
+  out.t.upload += msSince(t0);
 
   // --- K SOSP updates (one fused launch) ------------------------------------------
   t0 = std::chrono::steady_clock::now();
@@ -225,7 +267,7 @@ int runPipeline(mosp_workspace *ws, const PipelineIn &in, PipelineOut &out, std:
       dp[k] = dParent + static_cast<size_t>(k) * n;
     }
     const int st = mosp_sosp_update_multi(ws, n, m, K, dOutRow, dOutCol, outW, dInRow, dInCol, inW,
-                                          cf, ct, nc, dHeads, in.b.nIns, in.source, delta.data(),
+                                          cf, ct, nc, dInsTo, in.b.nIns, in.source, delta.data(),
                                           maxWeight.data(), dd, dp, out.stats.data(), nullptr);
     if (st != MOSP_OK) {
       err = mosp_last_error();
@@ -356,6 +398,7 @@ bool mospUpdateWithCosts(const CsrGraph &original, ChangeBatch &batch,
   in.pref = options.preferences.empty() ? nullptr : options.preferences.data();
   in.delta = options.delta;
   in.costs = costs != nullptr;
+  in.wantUpdated = true;
   if (costs != nullptr) costs->assign(static_cast<size_t>(n) * KG, DISTANCE_INF);
   result.distances.resize(kn);
   result.parents.resize(kn);

@@ -71,6 +71,8 @@ _SIGS = {
     "mosp_workspace_last_phases": (_i, [_p, _i, C.POINTER(C.c_ulonglong)]),
     "mosp_workspace_loop_profile": (_i, [_p, _i, C.POINTER(C.c_ulonglong), _llp, _llp]),
     "mosp_build_device_graph": (_i, [_p, _i, _i, _i, _p, _p, _p, _p, _p, _p, _p, _p]),
+    "mosp_apply_batch_device": (_i, [_p, _i, _i, _i, _p, _p, _p, _i, _p, _p, _p, _i, _p, _p, _p, _p, _p,
+                                     _ll, _ip, _p, _llp, _llp, _p]),
     "mosp_sosp_update": (_i, [_p, _i, _i, _p, _p, _p, _p, _p, _p, _p, _p, _i, _p, _i, _i, _ll, _ll,
                               _p, _p, C.POINTER(SospStats), _p]),
     "mosp_sosp_update_multi": (_i, [_p, _i, _i, _i, _p, _p, C.POINTER(_p), _p, _p, C.POINTER(_p),
@@ -447,6 +449,22 @@ class Workspace:
                                            arr(dist_list), arr(parent_list), stats, stream))
         return list(stats)
 
+    def apply_batch_device(self, n, K, m, row, col, w, ins_from, ins_to, ins_w, del_from, del_to,
+                           new_row, new_col, new_w, mask, stream=None):
+        """mosp_apply_batch_device: Step 1 on device buffers (edge-major
+        weights). Returns (new_m, max_weight[K], weight_sum[K])."""
+        nm = C.c_int()
+        mx = (C.c_longlong * K)()
+        sm = (C.c_longlong * K)()
+        n_ins = int(ins_from.numel()) if hasattr(ins_from, "numel") else len(ins_from)
+        n_del = int(del_from.numel()) if hasattr(del_from, "numel") else len(del_from)
+        cap = int(new_col.numel()) if hasattr(new_col, "numel") else len(new_col)
+        check(lib().mosp_apply_batch_device(self._h, n, K, m, _ptr(row), _ptr(col), _ptr(w), n_ins,
+                                            _ptr(ins_from), _ptr(ins_to), _ptr(ins_w), n_del, _ptr(del_from),
+                                            _ptr(del_to), _ptr(new_row), _ptr(new_col), _ptr(new_w), cap,
+                                            C.byref(nm), _ptr(mask), mx, sm, stream))
+        return nm.value, list(mx), list(sm)
+
     def sosp_from_scratch(self, n, m, out_row, out_col, out_w, source, delta, max_weight, dist, parent,
                           stream=None) -> SospStats:
         st = SospStats()
@@ -483,19 +501,25 @@ class Workspace:
         return (list(stats) if stats is not None else None), cst
 
     def update_host(self, graph_arrays, batch_arrays, init_dist, init_parent, K, source, pref=None,
-                    delta=0, costs=True):
-        """mosp_update_host: host buffers in, host buffers out."""
+                    delta=0, costs=True, out=None):
+        """mosp_update_host: host buffers in, host buffers out. `out` may hold
+        preallocated (e.g. pinned) result arrays (dist[K*n], parent[K*n],
+        comb_dist[n], comb_parent[n], costs[n*KG] or None)."""
         row, col, w = (_i32(x) for x in graph_arrays)
         n = len(row) - 1
         KG = w.shape[1]
         m = len(col)
         b = {k: _i32(v) for k, v in batch_arrays.items() if k != "mask"}
         init_dist, init_parent = _i64(init_dist), _i32(init_parent)
-        dist = np.empty(K * n, np.int64)
-        par = np.empty(K * n, np.int32)
-        cd = np.empty(n, np.int64)
-        cp = np.empty(n, np.int32)
-        cost = np.empty(n * KG, np.int64) if costs else None
+        if out is not None:
+            dist, par, cd, cp, cost = out
+            costs = cost is not None
+        else:
+            dist = np.empty(K * n, np.int64)
+            par = np.empty(K * n, np.int32)
+            cd = np.empty(n, np.int64)
+            cp = np.empty(n, np.int32)
+            cost = np.empty(n * KG, np.int64) if costs else None
         pa = None if pref is None else (C.c_int * K)(*pref)
         t = Timings()
         check(lib().mosp_update_host(self._h, n, KG, m, _ptr(row), _ptr(col), _ptr(w), len(b["ins_from"]),
