@@ -75,7 +75,7 @@ typedef struct mosp_combine_stats {
 /* Stage times of mosp_update_host, milliseconds (reference MospTimings,
  * headers/mospUpdate.cuh:35-46). */
 typedef struct mosp_timings {
-  double apply_batch;  /* host: apply the batch to the CSR */
+  double apply_batch;  /* GPU: apply the batch (Step 1), masks, change lists */
   double upload;       /* graph, trees and batch to the GPU */
   double objectives;   /* GPU: the K SOSP updates (one fused launch) */
   double combined;     /* GPU: combined graph + its SOSP tree */
@@ -127,6 +127,17 @@ void mosp_workspace_destroy(mosp_workspace *ws);
 /* Reserve scratch for K objectives of graphs with up to n vertices
  * (no-op if large enough). */
 int mosp_workspace_reserve(mosp_workspace *ws, int n, int K);
+
+/* Batched instances: many independent graphs stored as one disjoint union
+ * (vertex ids offset per instance) are updated by single launches when the
+ * workspace knows every instance's root. After this call every entry point
+ * that takes a `source` treats all `count` distinct vertices as roots
+ * (distance 0, parent -1; the `source` argument must be one of them), so
+ * each instance's trees, combined graph and costs are its own. count <= 1
+ * returns to single-source runs. No counterpart in the reference, which
+ * runs one instance per call. */
+int mosp_workspace_set_sources(mosp_workspace *ws, const int *h_sources,
+                               int count);
 
 /* Bound on every device-side wait of the persistent kernels (default
  * 10000 ms). A run that exceeds it stops and returns MOSP_ERR_TIMEOUT. */

@@ -10,6 +10,7 @@
 #include <cstring>
 #include <numeric>
 #include <string>
+#include <vector>
 
 #include "engine.h"
 #include "mosp_b200.h"
@@ -92,6 +93,10 @@ struct mosp_workspace {
   // Step 1 scratch (mosp_apply_batch_device)
   void *applyScratch = nullptr;
   size_t applyBytes = 0;
+  // roots of batched runs (mosp_workspace_set_sources): sorted, > 1 entries
+  std::vector<int> hostSources;
+  int *sources = nullptr;
+  int nSources = 0;
 };
 
 namespace {
@@ -276,7 +281,19 @@ int engineFlags() {
   return flags;
 }
 
+/// A source argument must be one of the workspace's roots in batched mode.
+int checkRoot(mosp_workspace *ws, int source) {
+  if (ws->nSources > 1 &&
+      !std::binary_search(ws->hostSources.begin(), ws->hostSources.end(), source)) {
+    return fail(MOSP_ERR_INVALID, "Error: the source is not one of the workspace's roots "
+                                  "(mosp_workspace_set_sources).");
+  }
+  return MOSP_OK;
+}
+
 void fillLists(EngineParams &p, mosp_workspace *ws, int block) {
+  p.sources = ws->nSources > 1 ? ws->sources : nullptr;
+  p.nSources = ws->nSources > 1 ? ws->nSources : 0;
   p.flags = engineFlags();
   p.timeoutNs = ws->timeoutNs;
   p.genPtr = ws->gen;
@@ -402,7 +419,9 @@ int prepareUpdate(mosp_workspace *ws, const UpdateArgs &a, EngineParams &p, int 
       a.inRow == nullptr || (a.m > 0 && (a.outCol == nullptr || a.inCol == nullptr))) {
     return fail(MOSP_ERR_INVALID, "Error: invalid SOSP update arguments.");
   }
-  int st = reserveLists(ws, a.n, a.K);
+  int st = checkRoot(ws, a.source);
+  if (st != MOSP_OK) return st;
+  st = reserveLists(ws, a.n, a.K);
   if (st != MOSP_OK) return st;
   if ((st = reserveNear(ws, a.n, a.m, a.K)) != MOSP_OK) return st;
   std::memset(&p, 0, sizeof(p));
@@ -453,7 +472,9 @@ int prepareCombined(mosp_workspace *ws, int n, int K, const int *d_parents, cons
   if (scale == 0) {
     return fail(MOSP_ERR_INVALID, "Error: invalid preference vector (need K values >= 1).");
   }
-  int st = reserveLists(ws, n, 1);
+  int st = checkRoot(ws, source);
+  if (st != MOSP_OK) return st;
+  st = reserveLists(ws, n, 1);
   if (st != MOSP_OK) return st;
   if ((st = reserveCombined(ws, n, K)) != MOSP_OK) return st;
   if ((st = reserveNear(ws, n, static_cast<long long>(n) * K, 1)) != MOSP_OK) return st;
@@ -578,6 +599,7 @@ void mosp_workspace_destroy(mosp_workspace *ws) {
     if (p) cudaFree(p);
   }
   if (ws->applyScratch) cudaFree(ws->applyScratch);
+  if (ws->sources) cudaFree(ws->sources);
   for (cudaEvent_t e : ws->ev) {
     if (e) cudaEventDestroy(e);
   }
@@ -592,6 +614,30 @@ int mosp_workspace_reserve(mosp_workspace *ws, int n, int K) {
   if (n < 0 || K < 1 || K > kMaxK) return fail(MOSP_ERR_INVALID, "invalid reserve size");
   if ((st = reserveLists(ws, std::max(n, 1), K)) != MOSP_OK) return st;
   return reserveCombined(ws, std::max(n, 1), K);
+}
+
+int mosp_workspace_set_sources(mosp_workspace *ws, const int *h_sources, int count) {
+  int st = checkWorkspace(ws);
+  if (st != MOSP_OK) return st;
+  if (count < 0 || (count > 0 && h_sources == nullptr)) {
+    return fail(MOSP_ERR_INVALID, "Error: invalid root list.");
+  }
+  std::vector<int> roots(h_sources, h_sources + count);
+  std::sort(roots.begin(), roots.end());
+  if (std::adjacent_find(roots.begin(), roots.end()) != roots.end() ||
+      (count > 0 && roots.front() < 0)) {
+    return fail(MOSP_ERR_INVALID, "Error: the roots must be distinct vertex ids >= 0.");
+  }
+  if (ws->sources) cudaFree(ws->sources);
+  ws->sources = nullptr;
+  ws->nSources = 0;
+  ws->hostSources.clear();
+  if (count <= 1) return MOSP_OK;
+  if ((st = deviceAlloc(&ws->sources, count)) != MOSP_OK) return st;
+  MOSP_CUDA(cudaMemcpy(ws->sources, roots.data(), count * sizeof(int), cudaMemcpyHostToDevice));
+  ws->hostSources = std::move(roots);
+  ws->nSources = count;
+  return MOSP_OK;
 }
 
 int mosp_workspace_set_timeout_ms(mosp_workspace *ws, long long ms) {
@@ -840,6 +886,7 @@ int mosp_sosp_from_scratch(mosp_workspace *ws, int n, int m, const int *d_out_ro
       d_parent == nullptr) {
     return fail(MOSP_ERR_INVALID, "Error: invalid SSSP arguments.");
   }
+  if ((st = checkRoot(ws, source)) != MOSP_OK) return st;
   if ((st = reserveLists(ws, n, 1)) != MOSP_OK) return st;
   if ((st = reserveNear(ws, n, m, 1)) != MOSP_OK) return st;
   int bits = 0;
@@ -981,6 +1028,7 @@ int mosp_path_costs(mosp_workspace *ws, int n, int m, int KG, const int *d_out_r
       (m > 0 && (d_out_col == nullptr || d_out_w == nullptr))) {
     return fail(MOSP_ERR_INVALID, "Error: invalid path-cost arguments.");
   }
+  if ((st = checkRoot(ws, source)) != MOSP_OK) return st;
   if (n > ws->costN || KG > ws->costKG) {
     const long long nn = std::max<long long>(n, ws->costN);
     const int kk = std::max(KG, ws->costKG);
@@ -998,6 +1046,8 @@ int mosp_path_costs(mosp_workspace *ws, int n, int m, int KG, const int *d_out_r
   c.m = m;
   c.KG = KG;
   c.source = source;
+  c.sources = ws->nSources > 1 ? ws->sources : nullptr;
+  c.nSources = ws->nSources > 1 ? ws->nSources : 0;
   c.timeoutNs = ws->timeoutNs;
   c.outRow = d_out_row;
   c.outCol = d_out_col;

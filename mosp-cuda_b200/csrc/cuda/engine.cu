@@ -671,7 +671,9 @@ __device__ bool unpackResults(const EngineParams &P, const int *outRow,
       for (long long v = tid; v < n; v += T) {
         const u64 word = __ldcg(P.packed + ko + v);
         O.dist[v] = word == kInfWord ? kDistInf : static_cast<long long>(word);
-        O.parent[v] = (word == kInfWord || v == P.source) ? -1 : INT_MAX;
+        O.parent[v] = (word == kInfWord || isRoot(P.source, P.sources, P.nSources, static_cast<int>(v)))
+                          ? -1
+                          : INT_MAX;
       }
     }
   }
@@ -701,7 +703,7 @@ __device__ bool unpackResults(const EngineParams &P, const int *outRow,
       if (deg > 0 && deg <= kLaneRowMax) {
         for (int e = beg; e < end; ++e) {
           const int x = ldGraph<Mode>(outCol + e);
-          if (x != P.source &&
+          if (!isRoot(P.source, P.sources, P.nSources, x) &&
               du + static_cast<u64>(ldGraph<Mode>(w + e)) == __ldcg(P.packed + ko + x)) {
             atomicMin(O.parent + x, static_cast<int>(uu));
           }
@@ -716,7 +718,7 @@ __device__ bool unpackResults(const EngineParams &P, const int *outRow,
         const int eb = __shfl_sync(kFull, end, src);
         for (int e = bb + static_cast<int>(lane); e < eb; e += 32) {
           const int x = ldGraph<Mode>(outCol + e);
-          if (x != P.source &&
+          if (!isRoot(P.source, P.sources, P.nSources, x) &&
               db + static_cast<u64>(ldGraph<Mode>(w + e)) == __ldcg(P.packed + ko + x)) {
             atomicMin(O.parent + x, ub);
           }
@@ -983,7 +985,7 @@ __global__ void __launch_bounds__(kThreads, 1) sospEngine(const __grid_constant_
           c->invalid = 1;
           continue;
         }
-        if (v == P.source || __ldcg(P.val + ko + v) == -2) continue;
+        if (isRoot(P.source, P.sources, P.nSources, v) || __ldcg(P.val + ko + v) == -2) continue;
         if (atomicExch(P.stamp + ko + v, genBase) != genBase) {
           const int idx = warpAppend(&c->candCount[k]);
           P.cand[ko + idx] = v;
@@ -1173,7 +1175,7 @@ __device__ void scratchOrCombined(const EngineParams &P, Sync &epoch, int genBas
     if (!gridSync(c, epoch)) return;
     unsigned long long edges = 0, wsum = 0;
     for (long long v = tid; v < n; v += T) {
-      if (v == P.source) continue;
+      if (isRoot(P.source, P.sources, P.nSources, static_cast<int>(v))) continue;
       for (int k = 0; k < P.combK; ++k) {
         int p, w;
         if (combinedEdge(P, static_cast<int>(v), k, p, w)) {
@@ -1207,7 +1209,7 @@ __device__ void scratchOrCombined(const EngineParams &P, Sync &epoch, int genBas
     }
     if (!gridSync(c, epoch)) return;
     for (long long v = tid; v < n; v += T) {
-      if (v == P.source) continue;
+      if (isRoot(P.source, P.sources, P.nSources, static_cast<int>(v))) continue;
       for (int k = 0; k < P.combK; ++k) {
         int p, w;
         if (combinedEdge(P, static_cast<int>(v), k, p, w)) {
@@ -1240,17 +1242,22 @@ __device__ void scratchOrCombined(const EngineParams &P, Sync &epoch, int genBas
     // fall through to the SSSP from scratch
   }
 
-  // ---- SSSP from scratch: only the source is finite ------------------------
+  // ---- SSSP from scratch: only the source (the roots) is finite ------------
   for (int k = 0; k < K; ++k) {
     const Pk pk = pkOf(P.obj[k]);
     const long long ko = static_cast<long long>(k) * P.stride;
     for (long long v = tid; v < n; v += T) {
-      P.packed[ko + v] = v == P.source ? pk.pack(0, -1) : kInfWord;
+      P.packed[ko + v] =
+          isRoot(P.source, P.sources, P.nSources, static_cast<int>(v)) ? pk.pack(0, -1) : kInfWord;
+    }
+    const int roots = P.nSources > 1 ? P.nSources : 1;
+    for (long long i = tid; i < roots; i += T) {
+      const int r = P.nSources > 1 ? P.sources[i] : P.source;
+      P.inFar[ko + r] = 1;
+      P.farL0[ko + i] = r;
     }
     if (tid == 0) {
-      P.inFar[ko + P.source] = 1;
-      P.farL0[ko] = P.source;
-      c->farCount[k][0] = 1;
+      c->farCount[k][0] = roots;
       c->farMinC[k][0] = ~0ULL;  // minimum 0
     }
   }
@@ -1373,7 +1380,9 @@ __global__ void __launch_bounds__(kThreads, 1) pathCosts(const __grid_constant__
     if (deg <= kLaneRowMax) {
       for (int e = beg; e < end; ++e) {
         const int v = __ldg(C.outCol + e);
-        if (v != C.source && __ldg(C.parent + v) == u) atomicMin(C.edgeOf + v, e);
+        if (!isRoot(C.source, C.sources, C.nSources, v) && __ldg(C.parent + v) == u) {
+          atomicMin(C.edgeOf + v, e);
+        }
       }
     }
     while (big != 0) {
@@ -1384,7 +1393,9 @@ __global__ void __launch_bounds__(kThreads, 1) pathCosts(const __grid_constant__
       const int eb = __shfl_sync(kFull, end, src);
       for (int e = bb + static_cast<int>(lane); e < eb; e += 32) {
         const int v = __ldg(C.outCol + e);
-        if (v != C.source && __ldg(C.parent + v) == ub) atomicMin(C.edgeOf + v, e);
+        if (!isRoot(C.source, C.sources, C.nSources, v) && __ldg(C.parent + v) == ub) {
+          atomicMin(C.edgeOf + v, e);
+        }
       }
     }
   }
@@ -1392,7 +1403,7 @@ __global__ void __launch_bounds__(kThreads, 1) pathCosts(const __grid_constant__
   for (long long v = tid; v < n; v += T) {
     const int p = __ldg(C.parent + v);
     long long *acc = C.acc0 + v * KG;
-    if (v == C.source) {
+    if (isRoot(C.source, C.sources, C.nSources, static_cast<int>(v))) {
       C.anc0[v] = -1;
       for (int k = 0; k < KG; ++k) acc[k] = 0;
     } else if (p < 0 || p >= n) {

@@ -101,6 +101,11 @@ enum : int {
 /// Parameters of one engine launch (passed by value, < 4 KB).
 struct EngineParams {
   int n, m, K, source;
+  // A batched run (independent instances stored as one disjoint union)
+  // has one root per instance: `sources` holds them sorted, `source` is the
+  // first. nSources <= 1 means the single root `source`.
+  const int *sources;
+  int nSources;
   int mode, maxRounds, nHeads, flags;
   long long timeoutNs;
   int *genPtr;                 // stamp generation, advanced by every launch
@@ -139,6 +144,8 @@ struct BuildParams {
 /// Parameters of the MOSP path-cost kernel.
 struct CostParams {
   int n, m, KG, source;
+  const int *sources;  // sorted roots of a batched run (nSources > 1), else unused
+  int nSources;
   long long timeoutNs;
   const int *outRow, *outCol, *outW;  // outW: KG objective-major columns
   const int *parent;
@@ -208,6 +215,20 @@ size_t applyScratchBytes(long long n, long long m, long long nIns, long long nDe
 /// the original edges (2K values).
 cudaError_t applyBatchGpu(ApplyParams P, void *scratch, int sms, cudaStream_t s, int *hostCounters,
                           long long *hostStats);
+
+/// Whether v is a root: the source, or one of the sorted batched roots.
+__device__ __forceinline__ bool isRoot(int source, const int *sources, int nSources, int v) {
+  if (v == source) return true;
+  if (nSources <= 1) return false;
+  int lo = 0, hi = nSources;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    const int s = sources[mid];
+    if (s == v) return true;
+    if (s < v) lo = mid + 1; else hi = mid;
+  }
+  return false;
+}
 
 /// Sets the calling thread's last-error message of the C ABI
 /// (mosp_last_error) and returns `status`.

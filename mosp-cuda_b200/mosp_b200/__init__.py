@@ -64,6 +64,7 @@ _SIGS = {
     "mosp_workspace_reserve": (_i, [_p, _i, _i]),
     "mosp_workspace_set_timeout_ms": (_i, [_p, _ll]),
     "mosp_workspace_set_ctas_per_sm": (_i, [_p, _i]),
+    "mosp_workspace_set_sources": (_i, [_p, _ip, _i]),
     "mosp_workspace_grid": (_i, [_p, _ip]),
     "mosp_workspace_buffer": (_i, [_p, _i, C.c_ulonglong, C.POINTER(_p)]),
     "mosp_workspace_enable_timing": (_i, [_p, _i]),
@@ -464,6 +465,12 @@ class Workspace:
                                             _ptr(del_to), _ptr(new_row), _ptr(new_col), _ptr(new_w), cap,
                                             C.byref(nm), _ptr(mask), mx, sm, stream))
         return nm.value, list(mx), list(sm)
+
+    def set_sources(self, sources):
+        """Roots of a batched run (one per instance of a disjoint union);
+        an empty list or one root returns to single-source runs."""
+        arr = (C.c_int * max(len(sources), 1))(*[int(x) for x in sources])
+        check(lib().mosp_workspace_set_sources(self._h, arr, len(sources)))
 
     def sosp_from_scratch(self, n, m, out_row, out_col, out_w, source, delta, max_weight, dist, parent,
                           stream=None) -> SospStats:
