@@ -60,6 +60,10 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--verify", action="store_true", help="check the result against the oracle")
+    ap.add_argument("--workload", choices=["road", "batched"], default="road",
+                    help="road: the road-network update (default); batched: 256 grid-road instances in one "
+                         "launch against per-instance launches")
+    ap.add_argument("--instances", type=int, default=256, help="batched workload: number of instances")
     return ap.parse_args()
 
 
@@ -350,6 +354,197 @@ def cpu_baseline_port(row, col, w, upd, ba, ch, old_d, old_p, K, src, changed):
 
 
 # ---------------------------------------------------------------------------
+# batched workload: many independent instances in one launch per step
+# ---------------------------------------------------------------------------
+BATCHED_METRIC = "batched MOSP updates: instances/s (K SOSP updates + combined graph + its SSSP per instance)"
+
+
+def make_batched_workload(count):
+    """Grid-road instances as in the road workload at log-uniform sizes in
+    [1,000, 200,000] vertices (seeds 12345*1000+i); per instance a batch of
+    1-10% of its edges, 50% insertions, mode drawn from uniform, targeted,
+    increase, reweight (seeds 777*1000+i)."""
+    import mosp_b200 as mb
+    rng = np.random.default_rng(12345)
+    modes = ["uniform", "targeted", "increase", "reweight"]
+    out = []
+    for i in range(count):
+        target = float(np.exp(rng.uniform(np.log(1e3), np.log(2e5))))
+        side = max(8, int(round(np.sqrt(target))))
+        g = mb.HostGraph.grid_road(side, side, 0.70, 0.01, 3, 1, 100, 12345 * 1000 + i)
+        mode = modes[int(rng.integers(0, 4))]
+        changes = max(2, int(g.m * rng.uniform(0.01, 0.10)))
+        try:
+            b = mb.HostBatch.generate(g, changes, 50.0, mode, 0, False, 777 * 1000 + i, 0, 1, 100)
+        except mb.MospError:
+            mode = "uniform"
+            b = mb.HostBatch.generate(g, changes, 50.0, mode, 0, False, 777 * 1000 + i, 0, 1, 100)
+        out.append((g, b, mode))
+    return out
+
+
+def run_batched(args):
+    import torch
+    import mosp_b200 as mb
+    from mosp_b200 import batched as bt
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    K = 3
+    insts = make_batched_workload(args.instances)
+    garrs = [g.arrays() for g, _, _ in insts]
+    bas = [b.arrays() for _, b, _ in insts]
+    row, col, w, off = bt.union_graphs(garrs)
+    ub = bt.union_batches(bas, off)
+    roots = off[:-1].astype(np.int32)
+    ug = mb.HostGraph.from_arrays(row, col, w)
+    ubatch = mb.HostBatch.from_arrays(K, ub["ins_from"], ub["ins_to"], ub["ins_w"], ub["del_from"], ub["del_to"])
+    upd = mb.apply_batch(ug, ubatch)
+    uba = ubatch.arrays()
+    N, M = upd.n, upd.m
+    changed = int(ubatch.n_ins + ubatch.n_del)
+
+    ws = mb.Workspace(timeout_ms=60000)
+    ws.set_sources(roots)
+    # initial trees of every instance: one from-scratch launch per objective
+    dg0 = mb.DeviceGraph.upload(ws, ug)
+    d0 = torch.empty((K, N), dtype=torch.int64, device="cuda")
+    p0 = torch.empty((K, N), dtype=torch.int32, device="cuda")
+    for k in range(K):
+        ws.sosp_from_scratch(N, ug.m, dg0.out_row, dg0.out_col, dg0.out_w_col(k), int(roots[0]),
+                             mb.default_delta(ug.m, N, int(w[:, k].sum())), int(w[:, k].max()), d0[k], p0[k])
+    del dg0
+    dg = mb.DeviceGraph.upload(ws, upd)
+    ch = mb.changed_lists(uba, K)
+    cf = torch.from_numpy(np.concatenate([c[0] for c in ch])).cuda()
+    ct = torch.from_numpy(np.concatenate([c[1] for c in ch])).cuda()
+    coff = np.concatenate([[0], np.cumsum([len(c[0]) for c in ch])])
+    heads = torch.from_numpy(uba["ins_to"].astype(np.int32)).cuda()
+    maxw = [max(int(w[:, k].max()), int(uba["ins_w"][:, k].max())) for k in range(K)]
+    base_deltas = [mb.default_delta(ug.m, N, int(w[:, k].sum())) for k in range(K)]
+    dist_t, par_t = torch.empty_like(d0), torch.empty_like(p0)
+    cd = torch.empty(N, dtype=torch.int64, device="cuda")
+    cp = torch.empty(N, dtype=torch.int32, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+    def default_step():
+        ws.update_device(N, M, K, dg.out_row, dg.out_col, dg.out_w, dg.in_row, dg.in_col, dg.in_w, cf, ct, coff,
+                         heads, len(uba["ins_to"]), int(roots[0]), base_deltas, maxw, None, dist_t, par_t, cd, cp,
+                         want_stats=False)
+
+    dist_t.copy_(d0)
+    par_t.copy_(p0)
+    tuned, comb_delta, tuned_ms = ws.autotune_update(N, M, K, dg.out_row, dg.out_col, dg.out_w, dg.in_row,
+                                                     dg.in_col, dg.in_w, cf, ct, coff, heads,
+                                                     len(uba["ins_to"]), int(roots[0]), base_deltas, maxw, None,
+                                                     dist_t, par_t, cd, cp)
+
+    def batched_step():
+        ws.update_device(N, M, K, dg.out_row, dg.out_col, dg.out_w, dg.in_row, dg.in_col, dg.in_w, cf, ct, coff,
+                         heads, len(uba["ins_to"]), int(roots[0]), tuned, maxw, None, dist_t, par_t, cd, cp,
+                         want_stats=False)
+
+    # the plain form: one mosp_update_device per instance on its own graph
+    pws = mb.Workspace(timeout_ms=60000)
+    plain = []
+    for i, (g, b, _) in enumerate(insts):
+        ga, ba_i = garrs[i], bas[i]
+        u_i = mb.apply_batch(g, b)
+        ba_i = b.arrays()
+        dgi = mb.DeviceGraph.upload(pws, u_i)
+        chi = mb.changed_lists(ba_i, K)
+        cfi = torch.from_numpy(np.concatenate([c[0] for c in chi]).astype(np.int32)).cuda()
+        cti = torch.from_numpy(np.concatenate([c[1] for c in chi]).astype(np.int32)).cuda()
+        offi = np.concatenate([[0], np.cumsum([len(c[0]) for c in chi])])
+        hi = torch.from_numpy(ba_i["ins_to"].astype(np.int32)).cuda() if len(ba_i["ins_to"]) else \
+            torch.zeros(1, dtype=torch.int32, device="cuda")
+        mwi = [max(int(ga[2][:, k].max()), int(ba_i["ins_w"][:, k].max()) if len(ba_i["ins_w"]) else 1)
+               for k in range(K)]
+        dli = [mb.default_delta(g.m, g.n, int(ga[2][:, k].sum())) for k in range(K)]
+        lo, hi_ = int(off[i]), int(off[i + 1])
+        d0i = d0[:, lo:hi_].clone()
+        p0i = torch.where(p0[:, lo:hi_] >= 0, p0[:, lo:hi_] - lo, p0[:, lo:hi_]).contiguous()
+        plain.append(dict(n=u_i.n, m=u_i.m, dg=dgi, cf=cfi, ct=cti, off=offi, heads=hi, nh=len(ba_i["ins_to"]),
+                          maxw=mwi, deltas=dli, d0=d0i, p0=p0i, d=torch.empty_like(d0i), p=torch.empty_like(p0i),
+                          cd=torch.empty(u_i.n, dtype=torch.int64, device="cuda"),
+                          cp=torch.empty(u_i.n, dtype=torch.int32, device="cuda")))
+
+    def plain_step():
+        for x in plain:
+            dg_i = x["dg"]
+            pws.update_device(x["n"], x["m"], K, dg_i.out_row, dg_i.out_col, dg_i.out_w, dg_i.in_row, dg_i.in_col,
+                              dg_i.in_w, x["cf"], x["ct"], x["off"], x["heads"], x["nh"], 0, x["deltas"], x["maxw"],
+                              None, x["d"], x["p"], x["cd"], x["cp"], want_stats=False)
+
+    def restore(fn):
+        # each form restores only its own trees, so both results survive
+        if fn is plain_step:
+            for x in plain:
+                x["d"].copy_(x["d0"])
+                x["p"].copy_(x["p0"])
+        else:
+            dist_t.copy_(d0)
+            par_t.copy_(p0)
+        flush.zero_()
+
+    def timed(fn):
+        restore(fn)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        fn()
+        e.record(stream)
+        e.synchronize()
+        return s.elapsed_time(e)
+
+    # the batched form with the default widths and eager launches, then with
+    # the tuned widths replayed as a CUDA graph
+    for _ in range(max(args.warmup, 0)):
+        timed(default_step)
+    def_ms = [timed(default_step) for _ in range(max(1, min(args.steps, 3)))]
+    ws.set_combined_delta(comb_delta)
+    ws.use_graphs(True)
+    for _ in range(max(args.warmup, 0)):
+        timed(batched_step)
+        timed(plain_step)
+    clocks = ClockSampler(local)
+    bt_ms = [timed(batched_step) for _ in range(args.steps)]
+    pl_ms = [timed(plain_step) for _ in range(max(1, min(args.steps, 3)))]
+    clock = clocks.stop()
+    # the batched results equal the per-instance ones, instance by instance
+    same = True
+    dd, pp, cdd, cpp = dist_t.cpu().numpy(), par_t.cpu().numpy(), cd.cpu().numpy(), cp.cpu().numpy()
+    for i, x in enumerate(plain):
+        same &= np.array_equal(bt.split_vertices(dd, off, i), x["d"].cpu().numpy())
+        same &= np.array_equal(bt.split_vertices(pp, off, i, parents=True), x["p"].cpu().numpy())
+        same &= np.array_equal(bt.split_vertices(cdd, off, i), x["cd"].cpu().numpy())
+        same &= np.array_equal(bt.split_vertices(cpp, off, i, parents=True), x["cp"].cpu().numpy())
+    b_ms, p_ms = float(np.mean(bt_ms)), float(np.mean(pl_ms))
+    if rank == 0:
+        line = {"metric": BATCHED_METRIC, "value": round(len(insts) / (b_ms / 1000.0), 2), "unit": "instances/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(b_ms, 4),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+                "data": "synthetic",
+                "config": {"workload": f"{len(insts)} grid-road instances, n log-uniform in [1e3, 2e5], K=3 "
+                                       "U[1,100], per-instance batches of 1-10% of the edges, 50% insertions, "
+                                       "modes uniform/targeted/increase/reweight",
+                           "instances": len(insts), "vertices": N, "edges": M, "changes_applied": changed,
+                           "modes": {mname: sum(1 for _, _, mm in insts if mm == mname)
+                                     for mname in ("uniform", "targeted", "increase", "reweight")},
+                           "delta_default": base_deltas, "delta_tuned": tuned, "combined_delta_tuned": comb_delta,
+                           "cuda_graph": True, "l2": "flushed (256 MiB write) before every timed step"},
+                "plain": {"value": round(len(insts) / (p_ms / 1000.0), 2), "unit": "instances/s",
+                          "ms_per_step": round(p_ms, 3), "steps": len(pl_ms),
+                          "form": "one mosp_update_device per instance (default widths), sequential"},
+                "batched_default_widths_ms": round(float(np.mean(def_ms)), 4),
+                "speedup_vs_plain": round(p_ms / b_ms, 2), "results_equal_plain": bool(same),
+                "changed_edges_per_s": round(changed / (b_ms / 1000.0), 1),
+                "gpu_launches": 2 * args.steps, "graph_launches": ws.graph_launches(), "clocks": clock}
+        print(json.dumps(line), flush=True)
+    ws.close()
+    pws.close()
+
+
+# ---------------------------------------------------------------------------
 # reference arm: the reference's own CPU implementation of the path
 # ---------------------------------------------------------------------------
 def run_reference(args):
@@ -438,6 +633,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batched":
+        run_batched(args)
     else:
         run_ours(args)
 

@@ -139,6 +139,22 @@ int mosp_workspace_reserve(mosp_workspace *ws, int n, int K);
 int mosp_workspace_set_sources(mosp_workspace *ws, const int *h_sources,
                                int count);
 
+/* Near-far bucket width of the combined-graph step run by
+ * mosp_update_device (0 = the default heuristic of the reference,
+ * src/combinedGraphGpu.cu:310-312). Results do not depend on it; the
+ * autotuner (mosp_autotune_update) picks it. */
+int mosp_workspace_set_combined_delta(mosp_workspace *ws, long long delta);
+
+/* When on, mosp_update_device records its launch sequence (control-block
+ * clears, the update and combined launches, the status readback) as one
+ * CUDA graph and replays it while the launch parameters stay the same; it
+ * is captured again when they change. Per-launch timing
+ * (mosp_workspace_enable_timing) is not recorded in this mode.
+ * mosp_workspace_graph_launches counts the graph launches so far. No
+ * counterpart in the reference. */
+int mosp_workspace_use_graphs(mosp_workspace *ws, int on);
+int mosp_workspace_graph_launches(mosp_workspace *ws, int *count);
+
 /* Bound on every device-side wait of the persistent kernels (default
  * 10000 ms). A run that exceeds it stops and returns MOSP_ERR_TIMEOUT. */
 int mosp_workspace_set_timeout_ms(mosp_workspace *ws, long long ms);
@@ -344,6 +360,31 @@ int mosp_update_device(mosp_workspace *ws, int n, int m, int K,
                        long long *d_comb_dist, int *d_comb_parent,
                        mosp_sosp_stats *stats, mosp_combine_stats *cstats,
                        void *stream);
+
+/* Autotuner of the near-far widths: runs mosp_update_device on the given
+ * inputs with the update width scaled by 1/4 .. 8 around h_delta and the
+ * combined-graph width scaled by 1/2 .. 16 around its default, timing each
+ * launch with CUDA events (best of two runs), and returns the fastest
+ * per-objective widths (h_best_delta, K entries), the fastest combined
+ * width (*h_best_comb_delta, for mosp_workspace_set_combined_delta) and
+ * their summed launch time (*h_best_ms, may be NULL). The trees d_dist /
+ * d_parent are restored to their input values before returning; results of
+ * later updates do not depend on the widths chosen. It allocates a copy of
+ * the trees for the duration of the call. No counterpart in the reference
+ * (its width is the fixed heuristic of defaultDelta). */
+int mosp_autotune_update(mosp_workspace *ws, int n, int m, int K,
+                         const int *d_out_row, const int *d_out_col,
+                         const int *d_out_w, const int *d_in_row,
+                         const int *d_in_col, const int *d_in_w,
+                         const int *d_changed_from, const int *d_changed_to,
+                         const int *h_changed_offset,
+                         const int *d_insert_heads, int n_heads, int source,
+                         const long long *h_delta,
+                         const long long *h_max_weight, const int *h_pref,
+                         long long *d_dist, int *d_parent,
+                         long long *d_comb_dist, int *d_comb_parent,
+                         long long *h_best_delta, long long *h_best_comb_delta,
+                         float *h_best_ms, void *stream);
 
 /* ---------------------------------------------------------------------- */
 /* Whole MOSP update from host memory (the reference's in-memory pipeline)  */

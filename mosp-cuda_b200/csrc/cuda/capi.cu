@@ -97,6 +97,14 @@ struct mosp_workspace {
   std::vector<int> hostSources;
   int *sources = nullptr;
   int nSources = 0;
+  // near-far width of the combined step in mosp_update_device (0: default)
+  long long combDelta = 0;
+  // CUDA graph of mosp_update_device's launch sequence (mosp_workspace_use_graphs)
+  bool useGraphs = false;
+  cudaStream_t captureStream = nullptr;
+  cudaGraphExec_t graphExec = nullptr;
+  EngineParams graphPu{}, graphPc{};
+  int graphReplays = 0;
 };
 
 namespace {
@@ -356,6 +364,52 @@ int readControl(mosp_workspace *ws, int first, int count, cudaStream_t s) {
   return MOSP_OK;
 }
 
+/// mosp_update_device's launch sequence (clear control block 0, update
+/// launch, clear control block 1, combined launch, control blocks to the
+/// pinned host copy) as one CUDA graph: captured on the workspace's own
+/// stream the first time and again whenever the launch parameters change,
+/// replayed on `s` otherwise. The caller waits on `s`.
+int launchUpdateGraph(mosp_workspace *ws, const EngineParams &pu, const EngineParams &pc,
+                      cudaStream_t s) {
+  const bool same = ws->graphExec != nullptr &&
+                    std::memcmp(&ws->graphPu, &pu, sizeof(EngineParams)) == 0 &&
+                    std::memcmp(&ws->graphPc, &pc, sizeof(EngineParams)) == 0;
+  if (!same) {
+    if (ws->graphExec) {
+      cudaGraphExecDestroy(ws->graphExec);
+      ws->graphExec = nullptr;
+    }
+    if (ws->captureStream == nullptr) {
+      MOSP_CUDA(cudaStreamCreateWithFlags(&ws->captureStream, cudaStreamNonBlocking));
+    }
+    cudaStream_t c = ws->captureStream;
+    MOSP_CUDA(cudaStreamBeginCapture(c, cudaStreamCaptureModeThreadLocal));
+    cudaError_t err = cudaMemsetAsync(ws->ctl, 0, sizeof(EngineControl), c);
+    if (err == cudaSuccess) err = launchEngineEx(pu, ws->shape.engineCtas, c);
+    if (err == cudaSuccess) err = cudaMemsetAsync(ws->ctl + 1, 0, sizeof(EngineControl), c);
+    if (err == cudaSuccess) err = launchEngineEx(pc, ws->shape.engineCtas, c);
+    if (err == cudaSuccess) {
+      err = cudaMemcpyAsync(ws->hostCtl, ws->ctl, 2 * sizeof(EngineControl),
+                            cudaMemcpyDeviceToHost, c);
+    }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t endErr = cudaStreamEndCapture(c, &graph);
+    if (err == cudaSuccess) err = endErr;
+    if (err == cudaSuccess) err = cudaGraphInstantiate(&ws->graphExec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (err != cudaSuccess) {
+      cudaGetLastError();
+      ws->graphExec = nullptr;
+      return cudaFail(err, "capturing the update as a CUDA graph");
+    }
+    ws->graphPu = pu;
+    ws->graphPc = pc;
+  }
+  MOSP_CUDA(cudaGraphLaunch(ws->graphExec, s));
+  ++ws->graphReplays;
+  return MOSP_OK;
+}
+
 /// Device-side status of a finished run.
 int controlStatus(mosp_workspace *ws, const EngineControl &c) {
   if (c.status != 0) {
@@ -600,6 +654,8 @@ void mosp_workspace_destroy(mosp_workspace *ws) {
   }
   if (ws->applyScratch) cudaFree(ws->applyScratch);
   if (ws->sources) cudaFree(ws->sources);
+  if (ws->graphExec) cudaGraphExecDestroy(ws->graphExec);
+  if (ws->captureStream) cudaStreamDestroy(ws->captureStream);
   for (cudaEvent_t e : ws->ev) {
     if (e) cudaEventDestroy(e);
   }
@@ -637,6 +693,29 @@ int mosp_workspace_set_sources(mosp_workspace *ws, const int *h_sources, int cou
   MOSP_CUDA(cudaMemcpy(ws->sources, roots.data(), count * sizeof(int), cudaMemcpyHostToDevice));
   ws->hostSources = std::move(roots);
   ws->nSources = count;
+  return MOSP_OK;
+}
+
+int mosp_workspace_set_combined_delta(mosp_workspace *ws, long long delta) {
+  if (ws == nullptr || delta < 0) return fail(MOSP_ERR_INVALID, "invalid combined-graph delta");
+  ws->combDelta = delta;
+  return MOSP_OK;
+}
+
+int mosp_workspace_use_graphs(mosp_workspace *ws, int on) {
+  int st = checkWorkspace(ws);
+  if (st != MOSP_OK) return st;
+  ws->useGraphs = on != 0;
+  if (!ws->useGraphs && ws->graphExec) {
+    cudaGraphExecDestroy(ws->graphExec);
+    ws->graphExec = nullptr;
+  }
+  return MOSP_OK;
+}
+
+int mosp_workspace_graph_launches(mosp_workspace *ws, int *count) {
+  if (ws == nullptr || count == nullptr) return fail(MOSP_ERR_INVALID, "invalid arguments");
+  *count = ws->graphReplays;
   return MOSP_OK;
 }
 
@@ -985,20 +1064,25 @@ int mosp_update_device(mosp_workspace *ws, int n, int m, int K, const int *d_out
   if ((st = prepareUpdate(ws, a, pu, bits)) != MOSP_OK) return st;
   long long scale = 0;
   int cbits = 0;
-  if ((st = prepareCombined(ws, n, K, d_parent, h_pref, source, 0, d_comb_dist, d_comb_parent, pc,
-                            scale, cbits)) != MOSP_OK) {
+  if ((st = prepareCombined(ws, n, K, d_parent, h_pref, source, ws->combDelta, d_comb_dist,
+                            d_comb_parent, pc, scale, cbits)) != MOSP_OK) {
     return st;
   }
   cudaStream_t s = asStream(stream);
   if ((st = cleanLists(ws, s)) != MOSP_OK) return st;
   fillLists(pu, ws, 0);
   fillLists(pc, ws, 1);
-  if ((st = markEvent(ws, 0, s)) != MOSP_OK) return st;
-  if ((st = queueEngine(ws, pu, 0, s)) != MOSP_OK) return st;
-  if ((st = markEvent(ws, 1, s)) != MOSP_OK) return st;
-  if ((st = queueEngine(ws, pc, 1, s)) != MOSP_OK) return st;
-  if ((st = markEvent(ws, 2, s)) != MOSP_OK) return st;
-  if ((st = readControl(ws, 0, 2, s)) != MOSP_OK) return st;
+  if (ws->useGraphs) {
+    if ((st = launchUpdateGraph(ws, pu, pc, s)) != MOSP_OK) return st;
+    MOSP_CUDA(cudaStreamSynchronize(s));
+  } else {
+    if ((st = markEvent(ws, 0, s)) != MOSP_OK) return st;
+    if ((st = queueEngine(ws, pu, 0, s)) != MOSP_OK) return st;
+    if ((st = markEvent(ws, 1, s)) != MOSP_OK) return st;
+    if ((st = queueEngine(ws, pc, 1, s)) != MOSP_OK) return st;
+    if ((st = markEvent(ws, 2, s)) != MOSP_OK) return st;
+    if ((st = readControl(ws, 0, 2, s)) != MOSP_OK) return st;
+  }
   readEvents(ws, &ws->lastUpdateMs, &ws->lastCombinedMs);
   if ((st = controlStatus(ws, ws->hostCtl[0])) != MOSP_OK) return st;
   if ((st = controlStatus(ws, ws->hostCtl[1])) != MOSP_OK) return st;
@@ -1011,11 +1095,105 @@ int mosp_update_device(mosp_workspace *ws, int n, int m, int K, const int *d_out
     cstats->edges = static_cast<int>(cc.sums[0]);
     cstats->reserved = 0;
     cstats->scale = scale;
-    cstats->delta = mosp_default_delta(static_cast<long long>(cc.sums[0]), n,
-                                       static_cast<long long>(cc.sums[1]));
+    cstats->delta = ws->combDelta > 0
+                        ? ws->combDelta
+                        : mosp_default_delta(static_cast<long long>(cc.sums[0]), n,
+                                             static_cast<long long>(cc.sums[1]));
     fillStats(cc, 0, cbits, &cstats->search);
   }
   return maybeResetGenerations(ws, std::max(cu.finalGen, cc.finalGen), s);
+}
+
+int mosp_autotune_update(mosp_workspace *ws, int n, int m, int K, const int *d_out_row,
+                         const int *d_out_col, const int *d_out_w, const int *d_in_row,
+                         const int *d_in_col, const int *d_in_w, const int *d_changed_from,
+                         const int *d_changed_to, const int *h_changed_offset,
+                         const int *d_insert_heads, int n_heads, int source,
+                         const long long *h_delta, const long long *h_max_weight,
+                         const int *h_pref, long long *d_dist, int *d_parent,
+                         long long *d_comb_dist, int *d_comb_parent, long long *h_best_delta,
+                         long long *h_best_comb_delta, float *h_best_ms, void *stream) {
+  int st = checkWorkspace(ws);
+  if (st != MOSP_OK) return st;
+  if (K < 1 || K > kMaxK || h_delta == nullptr || h_best_delta == nullptr ||
+      h_best_comb_delta == nullptr || d_dist == nullptr || d_parent == nullptr || n <= 0) {
+    return fail(MOSP_ERR_INVALID, "Error: invalid autotuner arguments.");
+  }
+  cudaStream_t s = asStream(stream);
+  const size_t kn = static_cast<size_t>(K) * n;
+  // the trees are updated in place: keep a copy and restore it before every
+  // trial and at the end
+  long long *saveDist = nullptr;
+  int *saveParent = nullptr;
+  if ((st = deviceAlloc(&saveDist, kn)) != MOSP_OK) return st;
+  if ((st = deviceAlloc(&saveParent, kn)) != MOSP_OK) {
+    cudaFree(saveDist);
+    return st;
+  }
+  struct Restore {
+    mosp_workspace *ws;
+    bool timing, graphs;
+    long long combDelta;
+    long long *d;
+    int *p;
+    ~Restore() {
+      ws->timing = timing;
+      ws->useGraphs = graphs;
+      ws->combDelta = combDelta;
+      cudaFree(d);
+      cudaFree(p);
+    }
+  } restore{ws, ws->timing, ws->useGraphs, ws->combDelta, saveDist, saveParent};
+  MOSP_CUDA(cudaMemcpyAsync(saveDist, d_dist, kn * sizeof(long long), cudaMemcpyDeviceToDevice, s));
+  MOSP_CUDA(cudaMemcpyAsync(saveParent, d_parent, kn * sizeof(int), cudaMemcpyDeviceToDevice, s));
+  ws->timing = true;
+  ws->useGraphs = false;
+  // (update factor, combined factor) pairs; the two launches are timed
+  // separately, so each factor list is searched independently
+  const double fu[] = {1.0, 0.5, 2.0, 4.0, 0.25, 8.0};
+  const double fc[] = {1.0, 2.0, 4.0, 8.0, 16.0, 0.5};
+  const int trials = 6;
+  float bestU = 1e30f, bestC = 1e30f;
+  double bestFu = 1.0;
+  long long combDefault = 0, bestComb = 0;
+  std::vector<long long> deltas(K);
+  for (int t = 0; t < trials; ++t) {
+    for (int k = 0; k < K; ++k) {
+      deltas[k] = std::max(1LL, static_cast<long long>(h_delta[k] * fu[t]));
+    }
+    ws->combDelta = t == 0 ? 0 : std::max(1LL, static_cast<long long>(combDefault * fc[t]));
+    float u = 1e30f, c = 1e30f;
+    for (int rep = 0; rep < 2; ++rep) {
+      MOSP_CUDA(cudaMemcpyAsync(d_dist, saveDist, kn * sizeof(long long), cudaMemcpyDeviceToDevice, s));
+      MOSP_CUDA(cudaMemcpyAsync(d_parent, saveParent, kn * sizeof(int), cudaMemcpyDeviceToDevice, s));
+      mosp_combine_stats cs{};
+      st = mosp_update_device(ws, n, m, K, d_out_row, d_out_col, d_out_w, d_in_row, d_in_col,
+                              d_in_w, d_changed_from, d_changed_to, h_changed_offset,
+                              d_insert_heads, n_heads, source, deltas.data(), h_max_weight, h_pref,
+                              d_dist, d_parent, d_comb_dist, d_comb_parent, nullptr, &cs, stream);
+      if (st != MOSP_OK) return st;
+      if (t == 0) combDefault = cs.delta;
+      u = std::min(u, ws->lastUpdateMs);
+      c = std::min(c, ws->lastCombinedMs);
+    }
+    if (u < bestU) {
+      bestU = u;
+      bestFu = fu[t];
+    }
+    if (c < bestC) {
+      bestC = c;
+      bestComb = t == 0 ? combDefault : ws->combDelta;
+    }
+  }
+  for (int k = 0; k < K; ++k) {
+    h_best_delta[k] = std::max(1LL, static_cast<long long>(h_delta[k] * bestFu));
+  }
+  *h_best_comb_delta = bestComb;
+  if (h_best_ms) *h_best_ms = bestU + bestC;
+  MOSP_CUDA(cudaMemcpyAsync(d_dist, saveDist, kn * sizeof(long long), cudaMemcpyDeviceToDevice, s));
+  MOSP_CUDA(cudaMemcpyAsync(d_parent, saveParent, kn * sizeof(int), cudaMemcpyDeviceToDevice, s));
+  MOSP_CUDA(cudaStreamSynchronize(s));
+  return MOSP_OK;
 }
 
 int mosp_path_costs(mosp_workspace *ws, int n, int m, int KG, const int *d_out_row,

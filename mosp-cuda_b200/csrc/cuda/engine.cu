@@ -1534,6 +1534,24 @@ cudaError_t launchEngine(const EngineParams &p, int ctas, cudaStream_t s) {
   return cudaLaunchCooperativeKernel(fn, dim3(ctas), dim3(kThreads), args, kStageBytes, s);
 }
 
+cudaError_t launchEngineEx(const EngineParams &p, int ctas, cudaStream_t s) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(ctas);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = kStageBytes;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  switch (p.mode) {
+    case kModeUpdate: return cudaLaunchKernelEx(&cfg, sospEngine<kModeUpdate>, p);
+    case kModeScratch: return cudaLaunchKernelEx(&cfg, sospEngine<kModeScratch>, p);
+    default: return cudaLaunchKernelEx(&cfg, sospEngine<kModeCombined>, p);
+  }
+}
+
 cudaError_t launchBuild(const BuildParams &p, int ctas, cudaStream_t s) {
   void *args[] = {const_cast<BuildParams *>(&p)};
   return cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(buildGraph), dim3(ctas),

@@ -163,6 +163,9 @@ struct LaunchShape {
 };
 cudaError_t queryLaunchShape(int ctasPerSm, LaunchShape &shape);
 cudaError_t launchEngine(const EngineParams &p, int ctas, cudaStream_t s);
+/// The same cooperative launch through cudaLaunchKernelEx with the
+/// cooperative attribute, the form a CUDA graph can capture.
+cudaError_t launchEngineEx(const EngineParams &p, int ctas, cudaStream_t s);
 cudaError_t launchBuild(const BuildParams &p, int ctas, cudaStream_t s);
 cudaError_t launchCosts(const CostParams &p, int ctas, cudaStream_t s);
 cudaError_t launchBarrierProbe(EngineControl *ctl, long long timeoutNs,

@@ -65,6 +65,11 @@ _SIGS = {
     "mosp_workspace_set_timeout_ms": (_i, [_p, _ll]),
     "mosp_workspace_set_ctas_per_sm": (_i, [_p, _i]),
     "mosp_workspace_set_sources": (_i, [_p, _ip, _i]),
+    "mosp_workspace_set_combined_delta": (_i, [_p, _ll]),
+    "mosp_workspace_use_graphs": (_i, [_p, _i]),
+    "mosp_workspace_graph_launches": (_i, [_p, _ip]),
+    "mosp_autotune_update": (_i, [_p, _i, _i, _i, _p, _p, _p, _p, _p, _p, _p, _p, _ip, _p, _i, _i,
+                                  _llp, _llp, _ip, _p, _p, _p, _p, _llp, _llp, C.POINTER(C.c_float), _p]),
     "mosp_workspace_grid": (_i, [_p, _ip]),
     "mosp_workspace_buffer": (_i, [_p, _i, C.c_ulonglong, C.POINTER(_p)]),
     "mosp_workspace_enable_timing": (_i, [_p, _i]),
@@ -465,6 +470,36 @@ class Workspace:
                                             _ptr(del_to), _ptr(new_row), _ptr(new_col), _ptr(new_w), cap,
                                             C.byref(nm), _ptr(mask), mx, sm, stream))
         return nm.value, list(mx), list(sm)
+
+    def set_combined_delta(self, delta):
+        check(lib().mosp_workspace_set_combined_delta(self._h, int(delta)))
+
+    def use_graphs(self, on=True):
+        check(lib().mosp_workspace_use_graphs(self._h, int(bool(on))))
+
+    def graph_launches(self) -> int:
+        c = C.c_int()
+        check(lib().mosp_workspace_graph_launches(self._h, C.byref(c)))
+        return c.value
+
+    def autotune_update(self, n, m, K, out_row, out_col, out_w, in_row, in_col, in_w, ch_from, ch_to,
+                        ch_offset, heads, n_heads, source, deltas, max_weights, pref, dist, parent,
+                        comb_dist, comb_parent, stream=None):
+        """mosp_autotune_update: returns (best deltas[K], best combined
+        delta, best summed launch ms); the trees are left unchanged."""
+        off = (C.c_int * (K + 1))(*[int(x) for x in ch_offset])
+        dl = (C.c_longlong * K)(*[int(x) for x in deltas])
+        mw = (C.c_longlong * K)(*[int(x) for x in max_weights])
+        pa = None if pref is None else (C.c_int * K)(*pref)
+        bd = (C.c_longlong * K)()
+        bc = C.c_longlong()
+        bm = C.c_float()
+        check(lib().mosp_autotune_update(self._h, n, m, K, _ptr(out_row), _ptr(out_col), _ptr(out_w),
+                                         _ptr(in_row), _ptr(in_col), _ptr(in_w), _ptr(ch_from), _ptr(ch_to),
+                                         off, _ptr(heads), n_heads, source, dl, mw, pa, _ptr(dist),
+                                         _ptr(parent), _ptr(comb_dist), _ptr(comb_parent), bd, C.byref(bc),
+                                         C.byref(bm), stream))
+        return list(bd), bc.value, bm.value
 
     def set_sources(self, sources):
         """Roots of a batched run (one per instance of a disjoint union);
