@@ -187,7 +187,7 @@ def run_ours(args):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device="cuda")
     stream = torch.cuda.current_stream()
 
-    def step(timed):
+    def step(timed, widths):
         dist_t.copy_(d0)
         par_t.copy_(p0)
         flush.zero_()
@@ -195,7 +195,7 @@ def run_ours(args):
             s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             s.record(stream)
         stats, cst = ws.update_device(n, upd.m, K, dg.out_row, dg.out_col, dg.out_w, dg.in_row, dg.in_col, dg.in_w,
-                                      cf, ct, off, heads, len(ba["ins_to"]), src, deltas, maxw, None, dist_t, par_t,
+                                      cf, ct, off, heads, len(ba["ins_to"]), src, widths, maxw, None, dist_t, par_t,
                                       cd, cp, stream=None)
         if timed:
             e.record(stream)
@@ -203,8 +203,23 @@ def run_ours(args):
             return s.elapsed_time(e), ws.last_timing(), stats, cst
         return None
 
+    # widths: the default heuristic (timed for comparison) and the autotuner's
+    # choice (the timed steps below), unless --delta fixes them
     for _ in range(max(args.warmup, 0)):
-        step(False)
+        step(False, deltas)
+    default_ms = [step(True, deltas)[0] for _ in range(3)]
+    comb_delta = 0
+    if args.delta <= 0:
+        dist_t.copy_(d0)
+        par_t.copy_(p0)
+        tuned, comb_delta, _ = ws.autotune_update(n, upd.m, K, dg.out_row, dg.out_col, dg.out_w, dg.in_row,
+                                                  dg.in_col, dg.in_w, cf, ct, off, heads, len(ba["ins_to"]), src,
+                                                  deltas, maxw, None, dist_t, par_t, cd, cp)
+        ws.set_combined_delta(comb_delta)
+    else:
+        tuned = deltas
+    for _ in range(max(args.warmup, 0)):
+        step(False, tuned)
     torch.cuda.synchronize()
     if pg:
         pg.barrier()
@@ -214,7 +229,7 @@ def run_ours(args):
     stats = cst = None
     wall0 = time.perf_counter()
     for _ in range(args.steps):
-        ms, (um, cm), stats, cst = step(True)
+        ms, (um, cm), stats, cst = step(True, tuned)
         step_ms.append(ms)
         upd_ms.append(um)
         comb_ms.append(cm)
@@ -309,9 +324,13 @@ def run_ours(args):
                 "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
                 "config": {"workload": WORKLOAD, "n": n, "m": upd.m, "K": K, "changes_applied": changed,
                            "inserts": batch.n_ins, "deletes": batch.n_del, "parallelism": f"replicas x{world}",
-                           "delta": deltas, "l2": "flushed (256 MiB write) before every timed step",
+                           "delta": tuned, "combined_delta": comb_delta or "default",
+                           "delta_default": deltas,
+                           "widths": "autotuned (mosp_autotune_update)" if args.delta <= 0 else "fixed by --delta",
+                           "l2": "flushed (256 MiB write) before every timed step",
                            "grid_ctas": ws.grid()},
                 "gpu_compute_ms": round(ms_per_step, 4),
+                "default_widths_ms_per_step": round(float(np.mean(default_ms)), 4),
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 2 * args.steps,
                 "clocks": clock, "wall_s_timed_loop": round(wall, 4), "phases_ms": phases,
                 "stats": {"invalidated": [s.invalidated for s in stats], "iterations": [s.iterations for s in stats],
