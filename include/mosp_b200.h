@@ -430,6 +430,81 @@ int mosp_debug_barrier_timeout(mosp_workspace *ws, long long timeout_ms,
 int mosp_debug_barrier_cost(mosp_workspace *ws, int rounds, int reads,
                             double *ns_per_round);
 
+/* ---------------------------------------------------------------------- */
+/* Serving: resident graphs, change batches from many clients                */
+/* ---------------------------------------------------------------------- */
+
+/* A server keeps graphs, their K SOSP trees and their combined (MOSP) tree
+ * in device memory and applies change batches that clients submit from any
+ * thread. Worker threads take the pending batches of one graph at a time
+ * (oldest first): batches that arrive while others run are picked up as
+ * soon as a worker and device memory are free; the pending batches of one
+ * graph are coalesced into one pass (each applied in order, then one engine
+ * update with the union of their change lists, which gives the same trees
+ * as applying them one by one); a pass starts only when the memory it may
+ * allocate fits in the free device memory minus `reserve_bytes` (unless no
+ * pass is running). The persistent launches of different workers run one
+ * at a time; their uploads, Step 1 kernels and downloads overlap. No
+ * counterpart in the reference, which runs one update per invocation. */
+typedef struct mosp_server mosp_server;
+
+typedef struct mosp_server_result {
+  int status;          /* MOSP_OK or the pass's error */
+  int graph;
+  long long version;   /* batches applied to the graph in the returned state */
+  int coalesced;       /* requests in the pass that served this one */
+  int reserved;
+  double queue_us;     /* submit -> pass start */
+  double latency_us;   /* submit -> result in host memory */
+  unsigned long long checksum; /* FNV-1a of the combined distances, parents */
+} mosp_server_result;
+
+typedef struct mosp_server_stats {
+  long long requests;  /* requests served */
+  long long passes;    /* GPU passes (a pass serves >= 1 request) */
+  long long changes;   /* changes applied */
+  long long deferred;  /* times a graph's pass waited for device memory */
+  int max_coalesced;
+  int reserved;
+  double busy_us;      /* summed pass durations over the workers */
+} mosp_server_stats;
+
+/* workers: 1..16 threads; max_coalesce: most requests per pass. */
+int mosp_server_create(int workers, long long reserve_bytes, int max_coalesce,
+                       mosp_server **out);
+void mosp_server_destroy(mosp_server *server);
+
+/* Upload a graph (host CSR, edge-major weights h_w[e*KG+k]) and compute its
+ * K canonical trees from `source` and its combined tree (Pref h_pref, K
+ * values or NULL) on the GPU; *graph_id identifies it. */
+int mosp_server_add_graph(mosp_server *server, int n, int KG, int m,
+                          const int *h_row, const int *h_col, const int *h_w,
+                          int K, int source, const int *h_pref, int *graph_id);
+
+/* Queue a change batch (host arrays, copied before returning) for a graph;
+ * *ticket identifies the request. Batches of one graph are applied in
+ * submission order. */
+int mosp_server_submit(mosp_server *server, int graph_id, int n_ins,
+                       const int *h_ins_from, const int *h_ins_to,
+                       const int *h_ins_w, int n_del, const int *h_del_from,
+                       const int *h_del_to, long long *ticket);
+
+/* Wait for a request: the graph's combined distances and parents (n each,
+ * either may be NULL) after the pass that served it, and its record. */
+int mosp_server_wait(mosp_server *server, long long ticket,
+                     long long *h_comb_dist, int *h_comb_parent,
+                     mosp_server_result *info);
+
+/* The graph's current state (after any running pass): its version, the K
+ * trees (K*n, objective-major) and the combined tree; any output may be
+ * NULL. */
+int mosp_server_read_graph(mosp_server *server, int graph_id,
+                           long long *version, long long *h_dist,
+                           int *h_parent, long long *h_comb_dist,
+                           int *h_comb_parent);
+
+int mosp_server_get_stats(mosp_server *server, mosp_server_stats *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -9,6 +9,10 @@
 
 namespace mospb200 {
 
+/// Sets the calling thread's last-error message of the C ABI
+/// (mosp_last_error) and returns `status` (defined with the C ABI).
+int recordFailure(int status, const char *message);
+
 /// Read-only view of a CSR graph (edge-major weights).
 struct GraphView {
   int n = 0, K = 0;

@@ -47,6 +47,18 @@ class CombineStats(C.Structure):
                 ("delta", C.c_longlong), ("search", SospStats)]
 
 
+class ServerResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("graph", C.c_int), ("version", C.c_longlong), ("coalesced", C.c_int),
+                ("reserved", C.c_int), ("queue_us", C.c_double), ("latency_us", C.c_double),
+                ("checksum", C.c_ulonglong)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("requests", C.c_longlong), ("passes", C.c_longlong), ("changes", C.c_longlong),
+                ("deferred", C.c_longlong), ("max_coalesced", C.c_int), ("reserved", C.c_int),
+                ("busy_us", C.c_double)]
+
+
 class Timings(C.Structure):
     _fields_ = [("apply_batch", C.c_double), ("upload", C.c_double), ("objectives", C.c_double),
                 ("combined", C.c_double), ("costs", C.c_double), ("download", C.c_double)]
@@ -97,6 +109,13 @@ _SIGS = {
                               _i, _ip, _ll, _p, _p, _p, _p, _p, C.POINTER(Timings)]),
     "mosp_debug_barrier_timeout": (_i, [_p, _ll, _ip]),
     "mosp_debug_barrier_cost": (_i, [_p, _i, _i, C.POINTER(C.c_double)]),
+    "mosp_server_create": (_i, [_i, _ll, _i, C.POINTER(_p)]),
+    "mosp_server_destroy": (None, [_p]),
+    "mosp_server_add_graph": (_i, [_p, _i, _i, _i, _p, _p, _p, _i, _i, _ip, _ip]),
+    "mosp_server_submit": (_i, [_p, _i, _i, _p, _p, _p, _i, _p, _p, _llp]),
+    "mosp_server_wait": (_i, [_p, _ll, _p, _p, C.POINTER(ServerResult)]),
+    "mosp_server_read_graph": (_i, [_p, _i, _llp, _p, _p, _p, _p]),
+    "mosp_server_get_stats": (_i, [_p, C.POINTER(ServerStats)]),
     # host side
     "mosp_graph_read": (_i, [C.c_char_p, C.c_char_p, C.POINTER(_p)]),
     "mosp_graph_write": (_i, [_p, C.c_char_p]),
@@ -580,6 +599,72 @@ class Workspace:
         st = C.c_int(-1)
         check(lib().mosp_debug_barrier_timeout(self._h, int(timeout_ms), C.byref(st)))
         return st.value
+
+
+class Server:
+    """mosp_server_*: resident graphs served by worker threads; change
+    batches from any thread, coalesced per graph, admitted by free device
+    memory."""
+
+    def __init__(self, workers=2, reserve_bytes=1 << 30, max_coalesce=64):
+        h = C.c_void_p()
+        check(lib().mosp_server_create(int(workers), int(reserve_bytes), int(max_coalesce), C.byref(h)))
+        self._h = h
+        self._n = {}
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            lib().mosp_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        if _lib is not None:
+            self.close()
+
+    def add_graph(self, graph_arrays, K, source=0, pref=None) -> int:
+        row, col, w = (_i32(x) for x in graph_arrays)
+        n, KG, m = len(row) - 1, w.shape[1], len(col)
+        gid = C.c_int()
+        pa = None if pref is None else (C.c_int * K)(*pref)
+        check(lib().mosp_server_add_graph(self._h, n, KG, m, _ptr(row), _ptr(col), _ptr(w), K, source, pa,
+                                          C.byref(gid)))
+        self._n[gid.value] = (n, K)
+        return gid.value
+
+    def submit(self, graph_id, batch_arrays) -> int:
+        b = {k: _i32(v) for k, v in batch_arrays.items() if k != "mask"}
+        t = C.c_longlong()
+        check(lib().mosp_server_submit(self._h, graph_id, len(b["ins_from"]), _ptr(b["ins_from"]), _ptr(b["ins_to"]),
+                                       _ptr(b["ins_w"]), len(b["del_from"]), _ptr(b["del_from"]), _ptr(b["del_to"]),
+                                       C.byref(t)))
+        return t.value
+
+    def wait(self, ticket, graph_id=None, want_result=True):
+        """(combined distances, combined parents, ServerResult); the arrays
+        are None when want_result is False."""
+        info = ServerResult()
+        cd = cp = None
+        if want_result:
+            n = self._n[graph_id][0]
+            cd = np.empty(n, np.int64)
+            cp = np.empty(n, np.int32)
+        check(lib().mosp_server_wait(self._h, int(ticket), _ptr(cd), _ptr(cp), C.byref(info)))
+        return cd, cp, info
+
+    def read_graph(self, graph_id):
+        n, K = self._n[graph_id]
+        v = C.c_longlong()
+        d = np.empty(K * n, np.int64)
+        p = np.empty(K * n, np.int32)
+        cd = np.empty(n, np.int64)
+        cp = np.empty(n, np.int32)
+        check(lib().mosp_server_read_graph(self._h, graph_id, C.byref(v), _ptr(d), _ptr(p), _ptr(cd), _ptr(cp)))
+        return v.value, d.reshape(K, n), p.reshape(K, n), cd, cp
+
+    def stats(self) -> ServerStats:
+        st = ServerStats()
+        check(lib().mosp_server_get_stats(self._h, C.byref(st)))
+        return st
 
 
 @dataclass
