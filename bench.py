@@ -60,7 +60,9 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--verify", action="store_true", help="check the result against the oracle")
-    ap.add_argument("--workload", choices=["road", "batched"], default="road",
+    ap.add_argument("--requests", type=int, default=400, help="serving workload: requests per arrival rate")
+    ap.add_argument("--rates", default="50,200,1000", help="serving workload: Poisson arrival rates (1/s)")
+    ap.add_argument("--workload", choices=["road", "batched", "serving"], default="road",
                     help="road: the road-network update (default); batched: 256 grid-road instances in one "
                          "launch against per-instance launches")
     ap.add_argument("--instances", type=int, default=256, help="batched workload: number of instances")
@@ -564,6 +566,134 @@ def run_batched(args):
 
 
 # ---------------------------------------------------------------------------
+# serving workload: resident graphs, Poisson arrivals of change batches
+# ---------------------------------------------------------------------------
+SERVING_METRIC = "served MOSP updates: sustained changed-edges/s with p50/p99 latency (arrival -> result on host)"
+
+
+def make_serving_graphs():
+    """8 grid-road graphs of 0.5M-2M vertices and 8 R-MAT graphs of scale
+    18-20 (edge factor 16), K = 4, weights U[1,1000] (seeds 12345*1000+i)."""
+    import mosp_b200 as mb
+    rng = np.random.default_rng(12345)
+    graphs = []
+    for i in range(8):
+        side = int(round(np.sqrt(rng.uniform(0.5e6, 2.0e6) / 0.97)))
+        graphs.append(("grid", mb.HostGraph.grid_road(side, side, 0.70, 0.01, 4, 1, 1000, 12345 * 1000 + i)))
+    for i, scale in enumerate([18, 18, 18, 19, 19, 19, 20, 20]):
+        graphs.append((f"rmat{scale}", mb.HostGraph.rmat(scale, 16, 0.57, 0.19, 0.19, 4, 1, 1000, False,
+                                                        12345 * 1000 + 8 + i)))
+    return graphs
+
+
+def run_serving(args):
+    import threading
+
+    import mosp_b200 as mb
+
+    world, rank, local = dist_setup(args)
+    import torch
+    torch.cuda.set_device(local)
+    K, pref = 4, [1, 1, 2, 3]
+    graphs = make_serving_graphs()
+    garrs = [g.arrays() for _, g in graphs]
+    rates = [float(x) for x in args.rates.split(",")]
+    sources_of = [np.repeat(np.arange(len(r) - 1, dtype=np.int32), np.diff(r)) for r, _, _ in garrs]
+    rng = np.random.default_rng(777)
+    results = []
+    for rate in rates:
+        # the request stream: Poisson arrivals, a uniformly chosen graph,
+        # batch size log-uniform in [100, 100000]; half the changes insert
+        # random vertex pairs (weights U[1,1000]), half delete random edges
+        # of the original graph (a deletion of an edge already gone is a
+        # no-op)
+        count = args.requests
+        gaps = rng.exponential(1.0 / rate, count)
+        targets = rng.integers(0, len(graphs), count)
+        sizes = np.exp(rng.uniform(np.log(100), np.log(100000), count)).astype(int)
+        reqs = []
+        for j in range(count):
+            row, col, _ = garrs[targets[j]]
+            src = sources_of[targets[j]]
+            n = len(row) - 1
+            ni = int(sizes[j]) // 2
+            nd = int(sizes[j]) - ni
+            pick = rng.integers(0, len(col), nd)
+            reqs.append((int(targets[j]), {
+                "ins_from": rng.integers(0, n, ni).astype(np.int32), "ins_to": rng.integers(0, n, ni).astype(np.int32),
+                "ins_w": rng.integers(1, 1001, (ni, K)).astype(np.int32),
+                "del_from": src[pick].astype(np.int32), "del_to": col[pick].astype(np.int32)}))
+        changes = sum(len(b["ins_from"]) + len(b["del_from"]) for _, b in reqs)
+
+        def serve(workers, coalesce, paced):
+            srv = mb.Server(workers=workers, reserve_bytes=4 << 30, max_coalesce=coalesce)
+            ids = [srv.add_graph(ga, K, 0, pref) for ga in garrs]
+            infos = [None] * count
+            tickets = [None] * count
+            ready = threading.Semaphore(0)
+
+            def waiter():
+                for j in range(count):
+                    ready.acquire()
+                    infos[j] = srv.wait(tickets[j], ids[reqs[j][0]], want_result=False)[2]
+
+            th = threading.Thread(target=waiter)
+            th.start()
+            t0 = time.perf_counter()
+            due = t0
+            for j, (gi, b) in enumerate(reqs):
+                if paced:
+                    due += gaps[j]
+                    delay = due - time.perf_counter()
+                    if delay > 0:
+                        time.sleep(delay)
+                tickets[j] = srv.submit(ids[gi], b)
+                ready.release()
+            th.join()
+            wall = time.perf_counter() - t0
+            st = srv.stats()
+            srv.close()
+            return infos, wall, st
+
+        infos, wall, st = serve(workers=2, coalesce=64, paced=True)
+        # the plain form: one request per pass, one worker, same per-graph order
+        plain, plain_wall, pst = serve(workers=1, coalesce=1, paced=False)
+        plain_sum = {(targets[j], plain[j].version): plain[j].checksum for j in range(count)}
+        equal = all(plain_sum.get((targets[j], infos[j].version)) == infos[j].checksum for j in range(count))
+        lat = np.array([x.latency_us for x in infos]) / 1000.0
+        queue = np.array([x.queue_us for x in infos]) / 1000.0
+        results.append({"rate_per_s": rate, "requests": count, "changes": int(changes),
+                        "p50_ms": round(float(np.percentile(lat, 50)), 3),
+                        "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                        "mean_queue_ms": round(float(queue.mean()), 3),
+                        "offered_s": round(float(gaps.sum()), 3), "wall_s": round(wall, 3),
+                        "changed_edges_per_s": round(changes / wall, 1), "passes": st.passes,
+                        "max_coalesced": st.max_coalesced, "deferred_admissions": st.deferred,
+                        "pass_ms": {"apply": round(st.apply_us / 1000 / max(st.passes, 1), 3),
+                                    "engine": round(st.engine_us / 1000 / max(st.passes, 1), 3),
+                                    "result": round(st.result_us / 1000 / max(st.passes, 1), 3)},
+                        "plain_wall_s": round(plain_wall, 3),
+                        "plain_pass_ms": {"apply": round(pst.apply_us / 1000 / max(pst.passes, 1), 3),
+                                          "engine": round(pst.engine_us / 1000 / max(pst.passes, 1), 3),
+                                          "result": round(pst.result_us / 1000 / max(pst.passes, 1), 3)},
+                        "all_equal_plain": bool(equal)})
+    if rank == 0:
+        top = results[-1]
+        line = {"metric": SERVING_METRIC, "value": top["changed_edges_per_s"], "unit": "changed-edges/s",
+                "n_gpus": world, "steps": args.requests, "warmup": 0,
+                "ms_per_step": round(1000 * top["wall_s"] / top["requests"], 3), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+                "config": {"workload": "16 resident graphs (8 grid-road 0.5M-2M vertices, 8 R-MAT scale 18-20 ef16), "
+                                       "K=4 U[1,1000], Pref=(1,1,2,3); Poisson arrivals, uniform graph choice, "
+                                       "batches log-uniform in [100, 100000] changes, 50% insertions of random "
+                                       "pairs, 50% deletions of random original edges",
+                           "graphs": [{"kind": kind, "n": g.n, "m": g.m} for kind, g in graphs],
+                           "workers": 2, "max_coalesce": 64, "reserve_bytes": 4 << 30},
+                "rates": results}
+        print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
 # reference arm: the reference's own CPU implementation of the path
 # ---------------------------------------------------------------------------
 def run_reference(args):
@@ -654,6 +784,8 @@ def main():
         run_reference(args)
     elif args.workload == "batched":
         run_batched(args)
+    elif args.workload == "serving":
+        run_serving(args)
     else:
         run_ours(args)
 

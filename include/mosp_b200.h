@@ -439,9 +439,11 @@ int mosp_debug_barrier_cost(mosp_workspace *ws, int rounds, int reads,
  * thread. Worker threads take the pending batches of one graph at a time
  * (oldest first): batches that arrive while others run are picked up as
  * soon as a worker and device memory are free; the pending batches of one
- * graph are coalesced into one pass (each applied in order, then one engine
- * update with the union of their change lists, which gives the same trees
- * as applying them one by one); a pass starts only when the memory it may
+ * graph are coalesced into one pass of at most max_coalesce requests and
+ * 262,144 changes past its first request (merged into one batch up to the
+ * first batch that deletes an edge an earlier one inserted, then one
+ * engine update with the union of their change lists, which gives the
+ * same trees as applying them one by one); a pass starts only when the memory it may
  * allocate fits in the free device memory minus `reserve_bytes` (unless no
  * pass is running). The persistent launches of different workers run one
  * at a time; their uploads, Step 1 kernels and downloads overlap. No
@@ -464,9 +466,13 @@ typedef struct mosp_server_stats {
   long long passes;    /* GPU passes (a pass serves >= 1 request) */
   long long changes;   /* changes applied */
   long long deferred;  /* times a graph's pass waited for device memory */
+  long long applies;   /* Step 1 runs (merged batches; > passes on conflicts) */
   int max_coalesced;
   int reserved;
   double busy_us;      /* summed pass durations over the workers */
+  double apply_us;     /* of which: uploads, Step 1, change lists */
+  double engine_us;    /* graph build + update + combined (incl. lock wait) */
+  double result_us;    /* combined tree download and checksum */
 } mosp_server_stats;
 
 /* workers: 1..16 threads; max_coalesce: most requests per pass. */

@@ -39,6 +39,7 @@
 #include <string>
 #include <thread>
 #include <unordered_map>
+#include <unordered_set>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -49,6 +50,8 @@
 namespace {
 
 using Clock = std::chrono::steady_clock;
+
+constexpr long long kPassChanges = 262144;  // changes per coalesced pass (after the first request)
 
 double usBetween(Clock::time_point a, Clock::time_point b) {
   return std::chrono::duration<double, std::micro>(b - a).count();
@@ -169,18 +172,20 @@ struct Staging {
   }
 };
 
+/// Checksum of a combined tree: FNV-1a style xor-multiply over 64-bit
+/// words (the distances, then the parents two at a time).
 unsigned long long checksumOf(const long long *d, const int *p, int n) {
-  // FNV-1a over the bytes of both arrays
   unsigned long long h = 1469598103934665603ULL;
-  auto mix = [&h](const void *data, size_t bytes) {
-    const unsigned char *c = static_cast<const unsigned char *>(data);
-    for (size_t i = 0; i < bytes; ++i) {
-      h ^= c[i];
-      h *= 1099511628211ULL;
-    }
-  };
-  mix(d, static_cast<size_t>(n) * sizeof(long long));
-  mix(p, static_cast<size_t>(n) * sizeof(int));
+  for (int v = 0; v < n; ++v) {
+    h ^= static_cast<unsigned long long>(d[v]);
+    h *= 1099511628211ULL;
+  }
+  for (int v = 0; v < n; v += 2) {
+    const unsigned long long lo = static_cast<unsigned>(p[v]);
+    const unsigned long long hi = v + 1 < n ? static_cast<unsigned>(p[v + 1]) : 0ULL;
+    h ^= lo | (hi << 32);
+    h *= 1099511628211ULL;
+  }
   return h;
 }
 
@@ -269,13 +274,53 @@ int mosp_server::runPass(mosp_workspace *ws, cudaStream_t s, Staging &st, Graph 
   std::vector<long long> mx(KG, 1), sum(KG, 0);
   bool firstApply = true;
   int rc = MOSP_OK;
+  const Clock::time_point tStart = Clock::now();
   auto cuda = [&err](cudaError_t e, const char *what) {
     if (e == cudaSuccess) return MOSP_OK;
     cudaGetLastError();
     err = std::string("CUDA error: ") + cudaGetErrorString(e) + " (" + what + ")";
     return MOSP_ERR_CUDA;
   };
-  for (auto &r : group) {
+  // The group's batches merge into one batch (deletions of all, then
+  // insertions of all, each in submission order) up to the first batch
+  // that deletes an edge an earlier batch of the merge inserted: until
+  // then, applying the merge equals applying the batches one by one
+  // (later insertions win, appended edges keep their order, repeated
+  // deletions take successive occurrences). A conflict starts a new merge.
+  struct Merged {
+    std::vector<int> insFrom, insTo, insW, delFrom, delTo;
+  };
+  std::vector<Merged> merges(1);
+  {
+    std::unordered_set<unsigned long long> inserted;
+    auto key = [](int u, int v) {
+      return (static_cast<unsigned long long>(static_cast<unsigned>(u)) << 32) |
+             static_cast<unsigned>(v);
+    };
+    for (auto &q : group) {
+      bool conflict = false;
+      for (size_t i = 0; i < q->delFrom.size() && !conflict && !inserted.empty(); ++i) {
+        conflict = inserted.count(key(q->delFrom[i], q->delTo[i])) != 0;
+      }
+      if (conflict) {
+        merges.emplace_back();
+        inserted.clear();
+      }
+      Merged &mg = merges.back();
+      mg.insFrom.insert(mg.insFrom.end(), q->insFrom.begin(), q->insFrom.end());
+      mg.insTo.insert(mg.insTo.end(), q->insTo.begin(), q->insTo.end());
+      mg.insW.insert(mg.insW.end(), q->insW.begin(), q->insW.end());
+      mg.delFrom.insert(mg.delFrom.end(), q->delFrom.begin(), q->delFrom.end());
+      mg.delTo.insert(mg.delTo.end(), q->delTo.begin(), q->delTo.end());
+      for (size_t i = 0; i < q->insFrom.size(); ++i) inserted.insert(key(q->insFrom[i], q->insTo[i]));
+    }
+  }
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    stats.applies += static_cast<long long>(merges.size());
+  }
+  for (const Merged &merged : merges) {
+    const Merged *r = &merged;
     const long long nIns = static_cast<long long>(r->insFrom.size());
     const long long nDel = static_cast<long long>(r->delFrom.size());
     // stage the batch through pinned memory
@@ -401,6 +446,7 @@ int mosp_server::runPass(mosp_workspace *ws, cudaStream_t s, Staging &st, Graph 
   }
   std::vector<long long> delta(K);
   for (int k = 0; k < K; ++k) delta[k] = mosp_default_delta(g.m, n, g.weightSum[k]);
+  const Clock::time_point tEngine = Clock::now();
   {
     std::lock_guard<std::mutex> gpu(gpuLock);
     rc = mosp_build_device_graph(ws, n, static_cast<int>(g.m), KG, g.row[g.cur], g.col[g.cur],
@@ -417,6 +463,7 @@ int mosp_server::runPass(mosp_workspace *ws, cudaStream_t s, Staging &st, Graph 
     err = mosp_last_error();
     return rc;
   }
+  const Clock::time_point tResult = Clock::now();
   // the combined tree back to the host, through pinned staging
   auto res = std::make_shared<Result>();
   res->combDist.resize(n);
@@ -434,6 +481,13 @@ int mosp_server::runPass(mosp_workspace *ws, cudaStream_t s, Staging &st, Graph 
   std::memcpy(res->combParent.data(), st.host + static_cast<size_t>(n) * 8,
               static_cast<size_t>(n) * 4);
   res->checksum = checksumOf(res->combDist.data(), res->combParent.data(), n);
+  const Clock::time_point tDone = Clock::now();
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    stats.apply_us += usBetween(tStart, tEngine);
+    stats.engine_us += usBetween(tEngine, tResult);
+    stats.result_us += usBetween(tResult, tDone);
+  }
   g.version += static_cast<long long>(group.size());
   for (auto &r : group) {
     r->result = res;
@@ -464,7 +518,14 @@ void mosp_server::worker(int index) {
     });
     if (g == nullptr) break;  // stopping
     std::vector<std::shared_ptr<Request>> group;
+    // a pass takes up to maxCoalesce requests and, past its first request,
+    // no more than kPassChanges changes, which bounds its duration
+    long long passChanges = 0;
     while (!g->pending.empty() && static_cast<int>(group.size()) < maxCoalesce) {
+      const Request &q = *g->pending.front();
+      const long long c = static_cast<long long>(q.insFrom.size() + q.delFrom.size());
+      if (!group.empty() && passChanges + c > kPassChanges) break;
+      passChanges += c;
       group.push_back(g->pending.front());
       g->pending.pop_front();
     }

@@ -55,8 +55,10 @@ class ServerResult(C.Structure):
 
 class ServerStats(C.Structure):
     _fields_ = [("requests", C.c_longlong), ("passes", C.c_longlong), ("changes", C.c_longlong),
-                ("deferred", C.c_longlong), ("max_coalesced", C.c_int), ("reserved", C.c_int),
-                ("busy_us", C.c_double)]
+                ("deferred", C.c_longlong), ("applies", C.c_longlong), ("max_coalesced", C.c_int),
+                ("reserved", C.c_int),
+                ("busy_us", C.c_double), ("apply_us", C.c_double), ("engine_us", C.c_double),
+                ("result_us", C.c_double)]
 
 
 class Timings(C.Structure):

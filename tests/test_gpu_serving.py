@@ -40,7 +40,14 @@ def scenario():
             except mb.MospError:
                 b = mb.HostBatch.generate(hg, size, 50.0, "uniform", 0, False, 1000 * gi + j, 0, 1, 100)
             ba = b.arrays()
-            seq.append({k: ba[k] for k in ("ins_from", "ins_to", "ins_w", "del_from", "del_to")})
+            x = {k: ba[k] for k in ("ins_from", "ins_to", "ins_w", "del_from", "del_to")}
+            if j % 2 == 1 and len(seq[-1]["ins_from"]):
+                # delete some edges the previous batch inserted: a merged pass
+                # must split here to stay equal to one-by-one application
+                prev = seq[-1]
+                x["del_from"] = np.concatenate([x["del_from"], prev["ins_from"][:5]]).astype(np.int32)
+                x["del_to"] = np.concatenate([x["del_to"], prev["ins_to"][:5]]).astype(np.int32)
+            seq.append(x)
         batches.append(seq)
     # oracle states after 0..len(seq) batches applied one by one
     states = []
@@ -115,7 +122,7 @@ def serve(scenario, alone, workers=2):
 def test_serving_mixed_requests(scenario):
     st = serve(scenario, alone=False, workers=2)
     assert st.requests == sum(len(b) for b in scenario[3])
-    assert st.passes <= st.requests
+    assert st.passes <= st.requests and st.passes <= st.applies
 
 
 def test_serving_alone(scenario):
