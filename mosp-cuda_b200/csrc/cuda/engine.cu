@@ -207,7 +207,7 @@ enum : int { kDone = 0, kPush = 1, kSplit = 2 };
 // CTA and list instead of one per warp group on the relaxation's critical
 // path. Entries that do not fit the buffer take the direct global path.
 // ---------------------------------------------------------------------------
-constexpr int kStage = 4096;
+constexpr int kStage = 8192;
 
 struct StageHeader {
   int cap;                     // entries per list partition (kStage / (2K))

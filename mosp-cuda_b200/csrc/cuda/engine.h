@@ -20,7 +20,7 @@ namespace mospb200 {
 
 using u64 = unsigned long long;
 
-constexpr int kThreads = 512;                 // threads per CTA
+constexpr int kThreads = 1024;                // threads per CTA
 constexpr int kMaxK = MOSP_MAX_OBJECTIVES;    // objectives per launch
 constexpr u64 kInfWord = ~0ULL;               // packed INF (all ones)
 constexpr long long kDistInf = MOSP_DISTANCE_INF;
