@@ -214,12 +214,15 @@ def run_ours(args):
     if args.delta <= 0:
         dist_t.copy_(d0)
         par_t.copy_(p0)
-        tuned, comb_delta, _ = ws.autotune_update(n, upd.m, K, dg.out_row, dg.out_col, dg.out_w, dg.in_row,
-                                                  dg.in_col, dg.in_w, cf, ct, off, heads, len(ba["ins_to"]), src,
-                                                  deltas, maxw, None, dist_t, par_t, cd, cp)
+        tuned, comb_delta, _, rounds = ws.autotune_update(n, upd.m, K, dg.out_row, dg.out_col, dg.out_w,
+                                                          dg.in_row, dg.in_col, dg.in_w, cf, ct, off, heads,
+                                                          len(ba["ins_to"]), src, deltas, maxw, None, dist_t,
+                                                          par_t, cd, cp)
         ws.set_combined_delta(comb_delta)
+        ws.set_local_rounds(*rounds)
     else:
         tuned = deltas
+        rounds = (0, 2)
     for _ in range(max(args.warmup, 0)):
         step(False, tuned)
     torch.cuda.synchronize()
@@ -327,6 +330,7 @@ def run_ours(args):
                 "config": {"workload": WORKLOAD, "n": n, "m": upd.m, "K": K, "changes_applied": changed,
                            "inserts": batch.n_ins, "deletes": batch.n_del, "parallelism": f"replicas x{world}",
                            "delta": tuned, "combined_delta": comb_delta or "default",
+                           "local_rounds": {"update": rounds[0], "combined": rounds[1]},
                            "delta_default": deltas,
                            "widths": "autotuned (mosp_autotune_update)" if args.delta <= 0 else "fixed by --delta",
                            "l2": "flushed (256 MiB write) before every timed step",
@@ -455,10 +459,10 @@ def run_batched(args):
 
     dist_t.copy_(d0)
     par_t.copy_(p0)
-    tuned, comb_delta, tuned_ms = ws.autotune_update(N, M, K, dg.out_row, dg.out_col, dg.out_w, dg.in_row,
-                                                     dg.in_col, dg.in_w, cf, ct, coff, heads,
-                                                     len(uba["ins_to"]), int(roots[0]), base_deltas, maxw, None,
-                                                     dist_t, par_t, cd, cp)
+    tuned, comb_delta, tuned_ms, rounds = ws.autotune_update(N, M, K, dg.out_row, dg.out_col, dg.out_w,
+                                                             dg.in_row, dg.in_col, dg.in_w, cf, ct, coff, heads,
+                                                             len(uba["ins_to"]), int(roots[0]), base_deltas, maxw,
+                                                             None, dist_t, par_t, cd, cp)
 
     def batched_step():
         ws.update_device(N, M, K, dg.out_row, dg.out_col, dg.out_w, dg.in_row, dg.in_col, dg.in_w, cf, ct, coff,
@@ -523,6 +527,7 @@ def run_batched(args):
         timed(default_step)
     def_ms = [timed(default_step) for _ in range(max(1, min(args.steps, 3)))]
     ws.set_combined_delta(comb_delta)
+    ws.set_local_rounds(*rounds)
     ws.use_graphs(True)
     for _ in range(max(args.warmup, 0)):
         timed(batched_step)
@@ -552,6 +557,7 @@ def run_batched(args):
                            "modes": {mname: sum(1 for _, _, mm in insts if mm == mname)
                                      for mname in ("uniform", "targeted", "increase", "reweight")},
                            "delta_default": base_deltas, "delta_tuned": tuned, "combined_delta_tuned": comb_delta,
+                           "local_rounds_tuned": {"update": rounds[0], "combined": rounds[1]},
                            "cuda_graph": True, "l2": "flushed (256 MiB write) before every timed step"},
                 "plain": {"value": round(len(insts) / (p_ms / 1000.0), 2), "unit": "instances/s",
                           "ms_per_step": round(p_ms, 3), "steps": len(pl_ms),

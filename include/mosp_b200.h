@@ -145,6 +145,16 @@ int mosp_workspace_set_sources(mosp_workspace *ws, const int *h_sources,
  * autotuner (mosp_autotune_update) picks it. */
 int mosp_workspace_set_combined_delta(mosp_workspace *ws, long long delta);
 
+/* CTA-local expansion rounds of the near-far loop (0..16) for update
+ * launches (default 0) and for from-scratch and combined-graph launches
+ * (default 2): after its share of an iteration, each CTA expands the near
+ * entries it has just produced itself up to this many times before the grid
+ * barrier, so a frontier advances several hops per barrier (it pays on
+ * deep, sparse graphs such as the combined graph). Results do not depend on
+ * it; the autotuner picks both. No counterpart in the reference. */
+int mosp_workspace_set_local_rounds(mosp_workspace *ws, int update_rounds,
+                                    int scratch_rounds);
+
 /* When on, mosp_update_device records its launch sequence (control-block
  * clears, the update and combined launches, the status readback) as one
  * CUDA graph and replays it while the launch parameters stay the same; it
@@ -361,13 +371,17 @@ int mosp_update_device(mosp_workspace *ws, int n, int m, int K,
                        mosp_sosp_stats *stats, mosp_combine_stats *cstats,
                        void *stream);
 
-/* Autotuner of the near-far widths: runs mosp_update_device on the given
- * inputs with the update width scaled by 1/4 .. 8 around h_delta and the
- * combined-graph width scaled by 1/2 .. 16 around its default, timing each
- * launch with CUDA events (best of two runs), and returns the fastest
- * per-objective widths (h_best_delta, K entries), the fastest combined
- * width (*h_best_comb_delta, for mosp_workspace_set_combined_delta) and
- * their summed launch time (*h_best_ms, may be NULL). The trees d_dist /
+/* Autotuner of the near-far widths and local rounds: runs
+ * mosp_update_device on the given inputs with the update width scaled by
+ * 1/4 .. 8 around h_delta and 0..2 local rounds, and the combined-graph
+ * width scaled by 1/2 .. 16 around its default with 0..4 local rounds,
+ * timing each launch with CUDA events (best of two runs), and returns the
+ * fastest per-objective widths (h_best_delta, K entries), the fastest
+ * combined width (*h_best_comb_delta, for
+ * mosp_workspace_set_combined_delta), the fastest local rounds
+ * (h_best_rounds[0] update, [1] combined, for
+ * mosp_workspace_set_local_rounds; may be NULL) and their summed launch
+ * time (*h_best_ms, may be NULL). The trees d_dist /
  * d_parent are restored to their input values before returning; results of
  * later updates do not depend on the widths chosen. It allocates a copy of
  * the trees for the duration of the call. No counterpart in the reference
@@ -384,7 +398,7 @@ int mosp_autotune_update(mosp_workspace *ws, int n, int m, int K,
                          long long *d_dist, int *d_parent,
                          long long *d_comb_dist, int *d_comb_parent,
                          long long *h_best_delta, long long *h_best_comb_delta,
-                         float *h_best_ms, void *stream);
+                         int *h_best_rounds, float *h_best_ms, void *stream);
 
 /* ---------------------------------------------------------------------- */
 /* Whole MOSP update from host memory (the reference's in-memory pipeline)  */

@@ -99,6 +99,10 @@ struct mosp_workspace {
   int nSources = 0;
   // near-far width of the combined step in mosp_update_device (0: default)
   long long combDelta = 0;
+  // CTA-local expansion rounds per near-far iteration: update launches,
+  // and from-scratch / combined-graph launches
+  int roundsUpdate = 0;
+  int roundsScratch = 2;
   // CUDA graph of mosp_update_device's launch sequence (mosp_workspace_use_graphs)
   bool useGraphs = false;
   cudaStream_t captureStream = nullptr;
@@ -300,6 +304,7 @@ int checkRoot(mosp_workspace *ws, int source) {
 }
 
 void fillLists(EngineParams &p, mosp_workspace *ws, int block) {
+  p.localRounds = p.mode == kModeUpdate ? ws->roundsUpdate : ws->roundsScratch;
   p.sources = ws->nSources > 1 ? ws->sources : nullptr;
   p.nSources = ws->nSources > 1 ? ws->nSources : 0;
   p.flags = engineFlags();
@@ -699,6 +704,16 @@ int mosp_workspace_set_sources(mosp_workspace *ws, const int *h_sources, int cou
 int mosp_workspace_set_combined_delta(mosp_workspace *ws, long long delta) {
   if (ws == nullptr || delta < 0) return fail(MOSP_ERR_INVALID, "invalid combined-graph delta");
   ws->combDelta = delta;
+  return MOSP_OK;
+}
+
+int mosp_workspace_set_local_rounds(mosp_workspace *ws, int update_rounds, int scratch_rounds) {
+  if (ws == nullptr || update_rounds < 0 || update_rounds > 16 || scratch_rounds < 0 ||
+      scratch_rounds > 16) {
+    return fail(MOSP_ERR_INVALID, "invalid local rounds");
+  }
+  ws->roundsUpdate = update_rounds;
+  ws->roundsScratch = scratch_rounds;
   return MOSP_OK;
 }
 
@@ -1112,7 +1127,8 @@ int mosp_autotune_update(mosp_workspace *ws, int n, int m, int K, const int *d_o
                          const long long *h_delta, const long long *h_max_weight,
                          const int *h_pref, long long *d_dist, int *d_parent,
                          long long *d_comb_dist, int *d_comb_parent, long long *h_best_delta,
-                         long long *h_best_comb_delta, float *h_best_ms, void *stream) {
+                         long long *h_best_comb_delta, int *h_best_rounds, float *h_best_ms,
+                         void *stream) {
   int st = checkWorkspace(ws);
   if (st != MOSP_OK) return st;
   if (K < 1 || K > kMaxK || h_delta == nullptr || h_best_delta == nullptr ||
@@ -1134,34 +1150,47 @@ int mosp_autotune_update(mosp_workspace *ws, int n, int m, int K, const int *d_o
     mosp_workspace *ws;
     bool timing, graphs;
     long long combDelta;
+    int roundsUpdate, roundsScratch;
     long long *d;
     int *p;
     ~Restore() {
       ws->timing = timing;
       ws->useGraphs = graphs;
       ws->combDelta = combDelta;
+      ws->roundsUpdate = roundsUpdate;
+      ws->roundsScratch = roundsScratch;
       cudaFree(d);
       cudaFree(p);
     }
-  } restore{ws, ws->timing, ws->useGraphs, ws->combDelta, saveDist, saveParent};
+  } restore{ws, ws->timing, ws->useGraphs, ws->combDelta, ws->roundsUpdate, ws->roundsScratch,
+            saveDist, saveParent};
   MOSP_CUDA(cudaMemcpyAsync(saveDist, d_dist, kn * sizeof(long long), cudaMemcpyDeviceToDevice, s));
   MOSP_CUDA(cudaMemcpyAsync(saveParent, d_parent, kn * sizeof(int), cudaMemcpyDeviceToDevice, s));
   ws->timing = true;
   ws->useGraphs = false;
-  // (update factor, combined factor) pairs; the two launches are timed
-  // separately, so each factor list is searched independently
-  const double fu[] = {1.0, 0.5, 2.0, 4.0, 0.25, 8.0};
-  const double fc[] = {1.0, 2.0, 4.0, 8.0, 16.0, 0.5};
-  const int trials = 6;
+  // Trial t runs the update with (width factor, local rounds) uc[t] and the
+  // combined step with cc[t]; the two launches are timed separately, so the
+  // two lists are searched independently. Trial 0 gives the combined
+  // default width the factors apply to.
+  struct Choice {
+    double factor;
+    int rounds;
+  };
+  const Choice uc[] = {{1, 0}, {0.5, 0}, {2, 0}, {4, 0}, {1, 1}, {2, 1}, {0.25, 0}, {8, 0}, {2, 2}};
+  const Choice cc[] = {{1, 2}, {4, 2}, {16, 2}, {1, 0}, {4, 0}, {16, 0}, {4, 4}, {16, 4}, {8, 3}};
+  const int trials = 9;
   float bestU = 1e30f, bestC = 1e30f;
-  double bestFu = 1.0;
+  Choice bestUc = uc[0];
   long long combDefault = 0, bestComb = 0;
+  int bestCr = cc[0].rounds;
   std::vector<long long> deltas(K);
   for (int t = 0; t < trials; ++t) {
     for (int k = 0; k < K; ++k) {
-      deltas[k] = std::max(1LL, static_cast<long long>(h_delta[k] * fu[t]));
+      deltas[k] = std::max(1LL, static_cast<long long>(h_delta[k] * uc[t].factor));
     }
-    ws->combDelta = t == 0 ? 0 : std::max(1LL, static_cast<long long>(combDefault * fc[t]));
+    ws->roundsUpdate = uc[t].rounds;
+    ws->roundsScratch = cc[t].rounds;
+    ws->combDelta = t == 0 ? 0 : std::max(1LL, static_cast<long long>(combDefault * cc[t].factor));
     float u = 1e30f, c = 1e30f;
     for (int rep = 0; rep < 2; ++rep) {
       MOSP_CUDA(cudaMemcpyAsync(d_dist, saveDist, kn * sizeof(long long), cudaMemcpyDeviceToDevice, s));
@@ -1178,17 +1207,22 @@ int mosp_autotune_update(mosp_workspace *ws, int n, int m, int K, const int *d_o
     }
     if (u < bestU) {
       bestU = u;
-      bestFu = fu[t];
+      bestUc = uc[t];
     }
     if (c < bestC) {
       bestC = c;
       bestComb = t == 0 ? combDefault : ws->combDelta;
+      bestCr = cc[t].rounds;
     }
   }
   for (int k = 0; k < K; ++k) {
-    h_best_delta[k] = std::max(1LL, static_cast<long long>(h_delta[k] * bestFu));
+    h_best_delta[k] = std::max(1LL, static_cast<long long>(h_delta[k] * bestUc.factor));
   }
   *h_best_comb_delta = bestComb;
+  if (h_best_rounds) {
+    h_best_rounds[0] = bestUc.rounds;
+    h_best_rounds[1] = bestCr;
+  }
   if (h_best_ms) *h_best_ms = bestU + bestC;
   MOSP_CUDA(cudaMemcpyAsync(d_dist, saveDist, kn * sizeof(long long), cudaMemcpyDeviceToDevice, s));
   MOSP_CUDA(cudaMemcpyAsync(d_parent, saveParent, kn * sizeof(int), cudaMemcpyDeviceToDevice, s));

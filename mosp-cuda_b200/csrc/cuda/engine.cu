@@ -213,6 +213,9 @@ struct StageHeader {
   int cap;                     // entries per list partition (kStage / (2K))
   int pad;
   int count[2 * kMaxK];        // appends per list this iteration (may exceed cap)
+  int start[2 * kMaxK];        // entries before this were expanded by the CTA itself
+  int roundEnd[kMaxK];         // end of the near entries of the current local round
+  int roundTotal;              // entries of the current local round (0: no round)
   int base[2 * kMaxK];         // global start of this CTA's range
   u64 farMin[kMaxK];           // minimum distance appended to far (plain)
   long long expanded[kMaxK];   // non-stale expansions (statistics)
@@ -313,7 +316,7 @@ __device__ void flushStage(const EngineParams &P, const LoopShared &L, int wrSlo
   __syncthreads();
   const int t = threadIdx.x;
   if (t < 2 * K) {
-    const int staged = H.count[t] < H.cap ? H.count[t] : H.cap;
+    const int staged = (H.count[t] < H.cap ? H.count[t] : H.cap) - H.start[t];
     if (staged > 0) H.base[t] = atomicAdd(listTarget(P, L, t, wrSlot, nearWV, nearWD).counter, staged);
   }
   if (t < K && H.farMin[t] != kInfWord) {
@@ -321,12 +324,13 @@ __device__ void flushStage(const EngineParams &P, const LoopShared &L, int wrSlo
   }
   __syncthreads();
   for (int l = 0; l < 2 * K; ++l) {
-    const int staged = H.count[l] < H.cap ? H.count[l] : H.cap;
-    if (staged == 0) continue;
+    const int first = H.start[l];
+    const int staged = (H.count[l] < H.cap ? H.count[l] : H.cap) - first;
+    if (staged <= 0) continue;
     const Target tg = listTarget(P, L, l, wrSlot, nearWV, nearWD);
     const int b = H.base[l];
     for (int i = t; i < staged; i += blockDim.x) {
-      const StageEntry e = E[l * H.cap + i];
+      const StageEntry e = E[l * H.cap + first + i];
       tg.v[b + i] = e.v;
       if (tg.d != nullptr) tg.d[b + i] = e.d;
     }
@@ -343,6 +347,119 @@ __device__ __forceinline__ int slotOwner(int incl, int s) {
     if (probe <= s) lo += step;
   }
   return lo;
+}
+
+/// One warp expands up to 32 near entries, one per lane (u < 0: none):
+/// the edges of all lanes are spread over the warp, two slots per lane,
+/// with their loads and 64-bit atomicMin overlapped; every strict
+/// improvement is staged for the next near list or the far pile. All 32
+/// lanes call it.
+template <int Mode>
+__device__ __forceinline__ void expandWarp(const EngineParams &P, const LoopShared &L,
+                                           const int *outRow, const int *outCol,
+                                           const int *const *outWk, int k, int u, u64 du, int beg,
+                                           int deg, int wrSlot, int *nearWV, u64 *nearWD) {
+  StageHeader &H = stageHeader();
+  const unsigned lane = laneId();
+  const int K = P.K;
+  {
+    // statistics: one shared add per objective present in the warp
+    const unsigned live = __ballot_sync(kFull, u >= 0);
+    if (live != 0) {
+      const unsigned peers = __match_any_sync(kFull, u >= 0 ? k : -1);
+      if (u >= 0 && static_cast<int>(lane) == __ffs(peers) - 1) {
+        atomicAdd(reinterpret_cast<unsigned long long *>(&H.expanded[k]),
+                  static_cast<unsigned long long>(__popc(peers)));
+      }
+    }
+  }
+  if (__ballot_sync(kFull, deg > 0) == 0) return;
+  // rows above 2^20 edges: whole-warp striding, one row at a time
+  unsigned huge = __ballot_sync(kFull, deg > (1 << 20));
+  while (huge != 0) {
+    const int src = __ffs(huge) - 1;
+    huge &= huge - 1;
+    const int kb = __shfl_sync(kFull, k, src);
+    const int ub = __shfl_sync(kFull, u, src);
+    const u64 db = __shfl_sync(kFull, du, src);
+    const int bb = __shfl_sync(kFull, beg, src);
+    const int eb = bb + __shfl_sync(kFull, deg, src);
+    const ObjectiveArgs &O = P.obj[kb];
+    const Pk pk = pkOf(O);
+    const long long kob = static_cast<long long>(kb) * P.stride;
+    for (int e = bb + static_cast<int>(lane); e < eb; e += 32) {
+      const int w = ldGraph<Mode>(outCol + e);
+      const u64 nd = db + static_cast<u64>(ldGraph<Mode>(outWk[kb] + e));
+      if (w == P.source || nd > O.maxDist) continue;
+      const u64 old = atomicMin(P.packed + kob + w, pk.pack(nd, ub));
+      if (nd >= pk.dist(old)) continue;
+      if (nd < L.thr[kb]) {
+        stageAppend(P, L, kb, w, nd, wrSlot, nearWV, nearWD);
+      } else if (atomicExch(P.inFar + kob + w, 1) == 0) {
+        stageAppend(P, L, K + kb, w, nd, wrSlot, nearWV, nearWD);
+      }
+    }
+  }
+  if (deg > (1 << 20)) deg = 0;
+  int incl = deg;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const int o = __shfl_up_sync(kFull, incl, off);
+    if (static_cast<int>(lane) >= off) incl += o;
+  }
+  const int edges = __shfl_sync(kFull, incl, 31);
+  const int excl = incl - deg;
+  for (int s0 = 0; s0 < edges; s0 += 64) {
+    // two edge slots per lane, their loads and atomics overlapped
+    int sl[2], kk[2], uu[2], ee[2], ww[2], wt[2];
+    u64 dd[2], nd[2], old[2];
+    bool act[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      sl[h] = s0 + 32 * h + static_cast<int>(lane);
+      const int o = slotOwner(incl, sl[h]);
+      kk[h] = __shfl_sync(kFull, k, o);
+      uu[h] = __shfl_sync(kFull, u, o);
+      dd[h] = __shfl_sync(kFull, du, o);
+      ee[h] = __shfl_sync(kFull, beg, o) + sl[h] - __shfl_sync(kFull, excl, o);
+      act[h] = sl[h] < edges;
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      ww[h] = act[h] ? ldGraph<Mode>(outCol + ee[h]) : 0;
+      wt[h] = act[h] ? ldGraph<Mode>(outWk[kk[h]] + ee[h]) : 0;
+    }
+    u64 cw[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      nd[h] = dd[h] + static_cast<u64>(wt[h]);
+      act[h] = act[h] && ww[h] != P.source && nd[h] <= P.obj[kk[h]].maxDist;
+      cw[h] = pkOf(P.obj[kk[h]]).pack(nd[h], uu[h]);
+    }
+    if (P.flags & kFlagPrecheck) {
+      u64 cur[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        cur[h] = act[h] ? __ldcg(P.packed + static_cast<long long>(kk[h]) * P.stride + ww[h]) : 0;
+      }
+#pragma unroll
+      for (int h = 0; h < 2; ++h) act[h] = act[h] && cw[h] < cur[h];
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      old[h] = act[h] ? atomicMin(P.packed + static_cast<long long>(kk[h]) * P.stride + ww[h], cw[h])
+                      : 0;
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      if (!act[h] || nd[h] >= pkOf(P.obj[kk[h]]).dist(old[h])) continue;
+      if (nd[h] < L.thr[kk[h]]) {
+        stageAppend(P, L, kk[h], ww[h], nd[h], wrSlot, nearWV, nearWD);
+      } else if (atomicExch(P.inFar + static_cast<long long>(kk[h]) * P.stride + ww[h], 1) == 0) {
+        stageAppend(P, L, K + kk[h], ww[h], nd[h], wrSlot, nearWV, nearWD);
+      }
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -387,7 +504,10 @@ __device__ bool nearFarLoop(const EngineParams &P, const int *outRow,
   for (;; ++it) {
     const int rdSlot = it % 3, wrSlot = (it + 1) % 3, clrSlot = (it + 2) % 3;
     const unsigned long long itStart = globalNs();
-    if (threadIdx.x < 2 * kMaxK) H.count[threadIdx.x] = 0;
+    if (threadIdx.x < 2 * kMaxK) {
+      H.count[threadIdx.x] = 0;
+      H.start[threadIdx.x] = 0;
+    }
     if (threadIdx.x < kMaxK) H.farMin[threadIdx.x] = kInfWord;
     if (threadIdx.x == 0) H.cap = kStage / (2 * K);
     if (warp == 0) {
@@ -495,104 +615,50 @@ __device__ bool nearFarLoop(const EngineParams &P, const int *outRow,
         beg = ldGraph<Mode>(outRow + u);
         deg = ldGraph<Mode>(outRow + u + 1) - beg;
       }
-      {
-        // statistics: one shared add per objective present in the warp
-        const unsigned live = __ballot_sync(kFull, u >= 0);
-        if (live != 0) {
-          const unsigned peers = __match_any_sync(kFull, u >= 0 ? k : -1);
-          if (u >= 0 && static_cast<int>(lane) == __ffs(peers) - 1) {
-            atomicAdd(reinterpret_cast<unsigned long long *>(&H.expanded[k]),
-                      static_cast<unsigned long long>(__popc(peers)));
-          }
+      expandWarp<Mode>(P, L, outRow, outCol, outWk, k, u, du, beg, deg, wrSlot, nearWV, nearWD);
+    }
+    // Local rounds: the CTA expands the near entries it has just staged
+    // itself, up to P.localRounds times while its partitions are at most
+    // half full, so a frontier advances several hops per grid barrier. An
+    // entry expanded here is not flushed; the last round's appends are.
+    // (Relaxations are monotone atomicMin, so expanding an entry earlier
+    // than the next iteration would cannot change the fixed point.)
+    for (int r = 0; r < P.localRounds; ++r) {
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        int tot = 0;
+        bool room = true;
+        for (int q = 0; q < K; ++q) {
+          const int end = H.count[q] < H.cap ? H.count[q] : H.cap;
+          H.roundEnd[q] = end;
+          tot += end - H.start[q];
+          room = room && H.count[q] <= H.cap / 2;
         }
+        H.roundTotal = room ? tot : 0;
       }
-      if (__ballot_sync(kFull, deg > 0) == 0) continue;
-      // rows above 2^20 edges: whole-warp striding, one row at a time
-      unsigned huge = __ballot_sync(kFull, deg > (1 << 20));
-      while (huge != 0) {
-        const int src = __ffs(huge) - 1;
-        huge &= huge - 1;
-        const int kb = __shfl_sync(kFull, k, src);
-        const int ub = __shfl_sync(kFull, u, src);
-        const u64 db = __shfl_sync(kFull, du, src);
-        const int bb = __shfl_sync(kFull, beg, src);
-        const int eb = bb + __shfl_sync(kFull, deg, src);
-        const ObjectiveArgs &O = P.obj[kb];
-        const Pk pk = pkOf(O);
-        const long long kob = static_cast<long long>(kb) * P.stride;
-        for (int e = bb + static_cast<int>(lane); e < eb; e += 32) {
-          const int w = ldGraph<Mode>(outCol + e);
-          const u64 nd = db + static_cast<u64>(ldGraph<Mode>(outWk[kb] + e));
-          if (w == P.source || nd > O.maxDist) continue;
-          const u64 old = atomicMin(P.packed + kob + w, pk.pack(nd, ub));
-          if (nd >= pk.dist(old)) continue;
-          if (nd < L.thr[kb]) {
-            stageAppend(P, L, kb, w, nd, wrSlot, nearWV, nearWD);
-          } else if (atomicExch(P.inFar + kob + w, 1) == 0) {
-            stageAppend(P, L, K + kb, w, nd, wrSlot, nearWV, nearWD);
+      __syncthreads();
+      const int tot = H.roundTotal;
+      if (tot == 0) break;
+      for (int b0 = warp * 32; b0 < tot; b0 += (blockDim.x >> 5) * 32) {
+        const int j = b0 + static_cast<int>(lane);
+        int kq = 0, uq = -1, begq = 0, degq = 0;
+        u64 dq = 0;
+        if (j < tot) {
+          int rem = j;
+          while (rem >= H.roundEnd[kq] - H.start[kq]) {
+            rem -= H.roundEnd[kq] - H.start[kq];
+            ++kq;
           }
+          const StageEntry e = stageEntries()[kq * H.cap + H.start[kq] + rem];
+          uq = e.v;
+          dq = e.d;
+          begq = ldGraph<Mode>(outRow + uq);
+          degq = ldGraph<Mode>(outRow + uq + 1) - begq;
         }
+        expandWarp<Mode>(P, L, outRow, outCol, outWk, kq, uq, dq, begq, degq, wrSlot, nearWV, nearWD);
       }
-      if (deg > (1 << 20)) deg = 0;
-      int incl = deg;
-#pragma unroll
-      for (int off = 1; off < 32; off <<= 1) {
-        const int o = __shfl_up_sync(kFull, incl, off);
-        if (static_cast<int>(lane) >= off) incl += o;
-      }
-      const int edges = __shfl_sync(kFull, incl, 31);
-      const int excl = incl - deg;
-      for (int s0 = 0; s0 < edges; s0 += 64) {
-        // two edge slots per lane, their loads and atomics overlapped
-        int sl[2], kk[2], uu[2], ee[2], ww[2], wt[2];
-        u64 dd[2], nd[2], old[2];
-        bool act[2];
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          sl[h] = s0 + 32 * h + static_cast<int>(lane);
-          const int o = slotOwner(incl, sl[h]);
-          kk[h] = __shfl_sync(kFull, k, o);
-          uu[h] = __shfl_sync(kFull, u, o);
-          dd[h] = __shfl_sync(kFull, du, o);
-          ee[h] = __shfl_sync(kFull, beg, o) + sl[h] - __shfl_sync(kFull, excl, o);
-          act[h] = sl[h] < edges;
-        }
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          ww[h] = act[h] ? ldGraph<Mode>(outCol + ee[h]) : 0;
-          wt[h] = act[h] ? ldGraph<Mode>(outWk[kk[h]] + ee[h]) : 0;
-        }
-        u64 cw[2];
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          nd[h] = dd[h] + static_cast<u64>(wt[h]);
-          act[h] = act[h] && ww[h] != P.source && nd[h] <= P.obj[kk[h]].maxDist;
-          cw[h] = pkOf(P.obj[kk[h]]).pack(nd[h], uu[h]);
-        }
-        if (P.flags & kFlagPrecheck) {
-          u64 cur[2];
-#pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            cur[h] = act[h] ? __ldcg(P.packed + static_cast<long long>(kk[h]) * P.stride + ww[h]) : 0;
-          }
-#pragma unroll
-          for (int h = 0; h < 2; ++h) act[h] = act[h] && cw[h] < cur[h];
-        }
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          old[h] = act[h] ? atomicMin(P.packed + static_cast<long long>(kk[h]) * P.stride + ww[h], cw[h])
-                          : 0;
-        }
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          if (!act[h] || nd[h] >= pkOf(P.obj[kk[h]]).dist(old[h])) continue;
-          if (nd[h] < L.thr[kk[h]]) {
-            stageAppend(P, L, kk[h], ww[h], nd[h], wrSlot, nearWV, nearWD);
-          } else if (atomicExch(P.inFar + static_cast<long long>(kk[h]) * P.stride + ww[h], 1) == 0) {
-            stageAppend(P, L, K + kk[h], ww[h], nd[h], wrSlot, nearWV, nearWD);
-          }
-        }
-      }
+      __syncthreads();
+      if (threadIdx.x < K) H.start[threadIdx.x] = H.roundEnd[threadIdx.x];
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) tWorked = globalNs();
     __syncthreads();

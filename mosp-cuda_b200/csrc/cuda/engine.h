@@ -107,6 +107,7 @@ struct EngineParams {
   const int *sources;
   int nSources;
   int mode, maxRounds, nHeads, flags;
+  int localRounds;  // CTA-local expansion rounds per near-far iteration (0: none)
   long long timeoutNs;
   int *genPtr;                 // stamp generation, advanced by every launch
   const int *outRow, *outCol, *inRow, *inCol;

@@ -81,9 +81,10 @@ _SIGS = {
     "mosp_workspace_set_sources": (_i, [_p, _ip, _i]),
     "mosp_workspace_set_combined_delta": (_i, [_p, _ll]),
     "mosp_workspace_use_graphs": (_i, [_p, _i]),
+    "mosp_workspace_set_local_rounds": (_i, [_p, _i, _i]),
     "mosp_workspace_graph_launches": (_i, [_p, _ip]),
     "mosp_autotune_update": (_i, [_p, _i, _i, _i, _p, _p, _p, _p, _p, _p, _p, _p, _ip, _p, _i, _i,
-                                  _llp, _llp, _ip, _p, _p, _p, _p, _llp, _llp, C.POINTER(C.c_float), _p]),
+                                  _llp, _llp, _ip, _p, _p, _p, _p, _llp, _llp, _ip, C.POINTER(C.c_float), _p]),
     "mosp_workspace_grid": (_i, [_p, _ip]),
     "mosp_workspace_buffer": (_i, [_p, _i, C.c_ulonglong, C.POINTER(_p)]),
     "mosp_workspace_enable_timing": (_i, [_p, _i]),
@@ -495,6 +496,9 @@ class Workspace:
     def set_combined_delta(self, delta):
         check(lib().mosp_workspace_set_combined_delta(self._h, int(delta)))
 
+    def set_local_rounds(self, update_rounds, scratch_rounds):
+        check(lib().mosp_workspace_set_local_rounds(self._h, int(update_rounds), int(scratch_rounds)))
+
     def use_graphs(self, on=True):
         check(lib().mosp_workspace_use_graphs(self._h, int(bool(on))))
 
@@ -507,7 +511,8 @@ class Workspace:
                         ch_offset, heads, n_heads, source, deltas, max_weights, pref, dist, parent,
                         comb_dist, comb_parent, stream=None):
         """mosp_autotune_update: returns (best deltas[K], best combined
-        delta, best summed launch ms); the trees are left unchanged."""
+        delta, best summed launch ms, best local rounds (update, combined));
+        the trees are left unchanged."""
         off = (C.c_int * (K + 1))(*[int(x) for x in ch_offset])
         dl = (C.c_longlong * K)(*[int(x) for x in deltas])
         mw = (C.c_longlong * K)(*[int(x) for x in max_weights])
@@ -515,12 +520,13 @@ class Workspace:
         bd = (C.c_longlong * K)()
         bc = C.c_longlong()
         bm = C.c_float()
+        br = (C.c_int * 2)()
         check(lib().mosp_autotune_update(self._h, n, m, K, _ptr(out_row), _ptr(out_col), _ptr(out_w),
                                          _ptr(in_row), _ptr(in_col), _ptr(in_w), _ptr(ch_from), _ptr(ch_to),
                                          off, _ptr(heads), n_heads, source, dl, mw, pa, _ptr(dist),
-                                         _ptr(parent), _ptr(comb_dist), _ptr(comb_parent), bd, C.byref(bc),
+                                         _ptr(parent), _ptr(comb_dist), _ptr(comb_parent), bd, C.byref(bc), br,
                                          C.byref(bm), stream))
-        return list(bd), bc.value, bm.value
+        return list(bd), bc.value, bm.value, (br[0], br[1])
 
     def set_sources(self, sources):
         """Roots of a batched run (one per instance of a disjoint union);

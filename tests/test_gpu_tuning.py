@@ -69,18 +69,36 @@ def test_autotuner_keeps_trees_and_results(ws, case):
     dist, par = dev(d0), dev(p0)
     cd = torch.empty(upd.n, dtype=torch.int64, device="cuda")
     cp = torch.empty(upd.n, dtype=torch.int32, device="cuda")
-    best, comb, ms = ws.autotune_update(upd.n, upd.m, K, dg.out_row, dg.out_col, dg.out_w, dg.in_row, dg.in_col,
+    best, comb, ms, rounds = ws.autotune_update(upd.n, upd.m, K, dg.out_row, dg.out_col, dg.out_w, dg.in_row, dg.in_col,
                                         dg.in_w, cf, ct, off, heads, len(ba["ins_to"]), 0, deltas, maxw, None,
                                         dist, par, cd, cp)
     assert len(best) == K and all(x >= 1 for x in best) and comb >= 1 and ms > 0
     assert np.array_equal(dist.cpu().numpy(), d0) and np.array_equal(par.cpu().numpy(), p0)
+    assert all(0 <= r <= 4 for r in rounds)
     ws.set_combined_delta(comb)
+    ws.set_local_rounds(*rounds)
     try:
         _, cst = run(ws, case, dg, cf, ct, off, heads, maxw, best, dist, par, cd, cp)
         assert cst.delta == comb
         check(exp, dist, par, cd, cp)
     finally:
         ws.set_combined_delta(0)
+        ws.set_local_rounds(0, 2)
+
+
+@pytest.mark.parametrize("rounds", [(0, 0), (1, 3), (4, 6)])
+def test_local_rounds_keep_results(ws, case, rounds):
+    K, g0, g, b, upd, ba, exp, d0, p0 = case
+    dg, cf, ct, off, heads, maxw, deltas = args_for(ws, case)
+    dist, par = dev(d0), dev(p0)
+    cd = torch.empty(upd.n, dtype=torch.int64, device="cuda")
+    cp = torch.empty(upd.n, dtype=torch.int32, device="cuda")
+    ws.set_local_rounds(*rounds)
+    try:
+        run(ws, case, dg, cf, ct, off, heads, maxw, deltas, dist, par, cd, cp)
+        check(exp, dist, par, cd, cp)
+    finally:
+        ws.set_local_rounds(0, 2)
 
 
 def test_graph_replay(ws, case):
