@@ -102,6 +102,10 @@ private:
 class Cursor {
 public:
   explicit Cursor(const std::string &t) : begin_(t.data()), p_(t.data()), end_(t.data() + t.size()) {}
+  /// Bytes [from, to) of t; line numbers still count from the start of t.
+  Cursor(const std::string &t, size_t from, size_t to)
+      : begin_(t.data()), p_(t.data() + from), end_(t.data() + to) {}
+  size_t offset() const { return static_cast<size_t>(p_ - begin_); }
   void blanks() {
     while (p_ < end_ && (*p_ == ' ' || *p_ == '\t' || *p_ == '\r')) ++p_;
   }
@@ -140,6 +144,83 @@ std::string at(const std::string &path, long long line) { return path + ":" + st
 
 bool validWeight(long long w) { return w >= 1 && w <= INT_MAX; }
 
+// --- parallel text I/O --------------------------------------------------------
+// Text files are parsed and formatted in chunks on all host cores: a chunk
+// boundary is moved to the next line start, every chunk is parsed on its
+// own, and the first error in file order is reported (the one a sequential
+// parse stops at). Formatting writes each chunk to its own buffer and the
+// buffers to the file in order, so the bytes equal a sequential writer's.
+
+int ioParts(size_t bytes) {
+  unsigned hc = std::thread::hardware_concurrency();
+  if (hc == 0) hc = 4;
+  const size_t byMb = std::max<size_t>(1, bytes >> 20);
+  return static_cast<int>(std::min<size_t>(std::min<unsigned>(hc, 64u), byMb));
+}
+
+/// parts + 1 offsets into text, each after a newline (or 0 / size).
+std::vector<size_t> lineChunks(const std::string &text, int parts) {
+  std::vector<size_t> b(static_cast<size_t>(parts) + 1, text.size());
+  b[0] = 0;
+  for (int i = 1; i < parts; ++i) {
+    size_t pos = std::max(b[i - 1], text.size() / parts * i);
+    while (pos < text.size() && pos > 0 && text[pos - 1] != '\n') ++pos;
+    b[i] = pos;
+  }
+  return b;
+}
+
+void parallelRun(int parts, const std::function<void(int)> &fn) {
+  if (parts <= 1) {
+    fn(0);
+    return;
+  }
+  std::vector<std::thread> threads;
+  threads.reserve(parts);
+  for (int i = 0; i < parts; ++i) threads.emplace_back([&fn, i] { fn(i); });
+  for (auto &t : threads) t.join();
+}
+
+/// First error of a chunked parse: byte offset (SIZE_MAX: none) and message
+/// builder given the line number.
+struct ChunkError {
+  size_t pos = SIZE_MAX;
+  std::function<std::string(long long)> message;
+  void set(size_t at, std::function<std::string(long long)> m) {
+    if (at < pos) {
+      pos = at;
+      message = std::move(m);
+    }
+  }
+};
+
+long long lineOf(const std::string &text, size_t pos) {
+  return 1 + static_cast<long long>(std::count(text.begin(), text.begin() + pos, '\n'));
+}
+
+/// Whitespace-separated tokens in text[from, to).
+size_t countTokens(const std::string &text, size_t from, size_t to) {
+  size_t tokens = 0;
+  bool inToken = false;
+  const char *p = text.data();
+  for (size_t i = from; i < to; ++i) {
+    const char ch = p[i];
+    const bool blank = ch == ' ' || ch == '\n' || ch == '\t' || ch == '\r';
+    tokens += (!blank && !inToken) ? 1 : 0;
+    inToken = !blank;
+  }
+  return tokens;
+}
+
+/// Exclusive prefix of per-chunk token counts (counted in parallel).
+std::vector<size_t> tokenOffsets(const std::string &text, const std::vector<size_t> &b) {
+  const int parts = static_cast<int>(b.size()) - 1;
+  std::vector<size_t> at(static_cast<size_t>(parts) + 1, 0);
+  parallelRun(parts, [&](int i) { at[i + 1] = countTokens(text, b[i], b[i + 1]); });
+  for (int i = 0; i < parts; ++i) at[i + 1] += at[i];
+  return at;
+}
+
 /// Whitespace-separated integers in [0, INT_MAX] (ids and offsets).
 bool parseIds(const std::string &path, std::vector<int> &out, std::string &err) {
   std::string text;
@@ -147,23 +228,39 @@ bool parseIds(const std::string &path, std::vector<int> &out, std::string &err) 
     err = "could not read " + path;
     return false;
   }
-  Cursor c(text);
-  out.clear();
-  out.reserve(text.size() / 4);
-  long long v = 0;
-  c.space();
-  while (!c.done()) {
-    if (!c.integer(v)) {
-      err = "invalid token at " + at(path, c.line());
-      return false;
-    }
-    if (v < 0 || v > INT_MAX) {
-      err = "value " + std::to_string(v) + " out of range [0, " + std::to_string(INT_MAX) +
-            "] at " + at(path, c.line());
-      return false;
-    }
-    out.push_back(static_cast<int>(v));
+  const int parts = ioParts(text.size());
+  const std::vector<size_t> b = lineChunks(text, parts);
+  // count the tokens first so that every chunk parses straight into place
+  const std::vector<size_t> start = tokenOffsets(text, b);
+  out.assign(start[parts], 0);
+  std::vector<ChunkError> errs(parts);
+  parallelRun(parts, [&](int i) {
+    Cursor c(text, b[i], b[i + 1]);
+    int *o = out.data() + start[i];
+    long long v = 0;
     c.space();
+    while (!c.done()) {
+      const size_t pos = c.offset();
+      if (!c.integer(v)) {
+        errs[i].set(pos, [path](long long line) { return "invalid token at " + path + ":" + std::to_string(line); });
+        return;
+      }
+      if (v < 0 || v > INT_MAX) {
+        errs[i].set(pos, [path, v](long long line) {
+          return "value " + std::to_string(v) + " out of range [0, " + std::to_string(INT_MAX) + "] at " +
+                 path + ":" + std::to_string(line);
+        });
+        return;
+      }
+      *o++ = static_cast<int>(v);
+      c.space();
+    }
+  });
+  for (int i = 0; i < parts; ++i) {
+    if (errs[i].pos != SIZE_MAX) {
+      err = errs[i].message(lineOf(text, errs[i].pos));
+      return false;
+    }
   }
   return true;
 }
@@ -177,40 +274,73 @@ bool parseValues(const std::string &path, std::vector<int> &w, int &K, long long
     err = "Could not read CSR values file " + path + ".";
     return false;
   }
-  Cursor c(text);
-  w.clear();
-  w.reserve(text.size() / 3);
+  const int parts = ioParts(text.size());
+  const std::vector<size_t> b = lineChunks(text, parts);
+  const std::vector<size_t> start = tokenOffsets(text, b);
+  w.assign(start[parts], 0);
+  std::vector<ChunkError> errs(parts);
+  std::vector<int> chunkK(parts, 0);
+  std::vector<size_t> firstLine(parts, SIZE_MAX);
+  std::vector<long long> chunkLines(parts, 0);
+  parallelRun(parts, [&](int i) {
+    Cursor c(text, b[i], b[i + 1]);
+    int *o = w.data() + start[i];
+    for (;;) {
+      c.blanks();
+      const size_t lineStart = c.offset();
+      int count = 0;
+      long long v = 0;
+      while (!c.done() && !c.eol()) {
+        const size_t at = c.offset();
+        if (!c.integer(v)) {
+          errs[i].set(at, [path](long long line) {
+            return "Invalid token in CSR values file at " + path + ":" + std::to_string(line) + ".";
+          });
+          return;
+        }
+        if (!validWeight(v)) {
+          errs[i].set(at, [path, v](long long line) {
+            return "CSR weight " + std::to_string(v) + " out of range [1, " + std::to_string(INT_MAX) +
+                   "] at " + path + ":" + std::to_string(line) + ".";
+          });
+          return;
+        }
+        *o++ = static_cast<int>(v);
+        ++count;
+        c.blanks();
+      }
+      if (count > 0) {
+        if (chunkK[i] == 0) {
+          chunkK[i] = count;
+          firstLine[i] = lineStart;
+        } else if (count != chunkK[i]) {
+          errs[i].set(c.offset(), [path](long long line) {
+            return "Inconsistent number of objectives at " + path + ":" + std::to_string(line) + ".";
+          });
+          return;
+        }
+        ++chunkLines[i];
+      }
+      if (c.done()) break;
+      c.next();
+    }
+  });
   K = 0;
   lines = 0;
-  for (;;) {
-    c.blanks();
-    int count = 0;
-    long long v = 0;
-    while (!c.done() && !c.eol()) {
-      if (!c.integer(v)) {
-        err = "Invalid token in CSR values file at " + at(path, c.line()) + ".";
-        return false;
-      }
-      if (!validWeight(v)) {
-        err = "CSR weight " + std::to_string(v) + " out of range [1, " +
-              std::to_string(INT_MAX) + "] at " + at(path, c.line()) + ".";
-        return false;
-      }
-      w.push_back(static_cast<int>(v));
-      ++count;
-      c.blanks();
+  for (int i = 0; i < parts; ++i) {
+    // a chunk whose lines have another width than the file's first line
+    // fails at its own first line, before any error inside the chunk
+    if (chunkK[i] != 0 && K != 0 && chunkK[i] != K) {
+      err = "Inconsistent number of objectives at " + path + ":" +
+            std::to_string(lineOf(text, firstLine[i])) + ".";
+      return false;
     }
-    if (count > 0) {
-      if (K == 0) {
-        K = count;
-      } else if (count != K) {
-        err = "Inconsistent number of objectives at " + at(path, c.line()) + ".";
-        return false;
-      }
-      ++lines;
+    if (errs[i].pos != SIZE_MAX) {
+      err = errs[i].message(lineOf(text, errs[i].pos));
+      return false;
     }
-    if (c.done()) break;
-    c.next();
+    if (K == 0) K = chunkK[i];
+    lines += chunkLines[i];
   }
   return true;
 }
@@ -281,6 +411,40 @@ bool csrArraysValid(const CsrGraph &g) {
 }  // namespace
 
 // ---------------------------------------------------------------------------
+
+namespace mospb200 {
+
+bool writeLinesParallel(const std::string &path, size_t count,
+                        const std::function<void(size_t, std::string &)> &line) {
+  makeParentDir(path);
+  FILE *f = std::fopen(path.c_str(), "wb");
+  if (f == nullptr) return false;
+  // chunks of about 64K lines, formatted in waves of one chunk per core
+  const int parts = static_cast<int>(std::max<size_t>(1, (count + 65535) >> 16));
+  std::vector<std::string> bufs(parts);
+  bool ok = true;
+  const int wave = ioParts(count * 8);
+  for (int w0 = 0; w0 < parts && ok; w0 += wave) {
+    const int w1 = std::min(parts, w0 + wave);
+    parallelRun(w1 - w0, [&](int j) {
+      const int i = w0 + j;
+      const size_t a = count * static_cast<size_t>(i) / parts;
+      const size_t z = count * static_cast<size_t>(i + 1) / parts;
+      std::string &out = bufs[i];
+      out.reserve((z - a) * 12);
+      for (size_t x = a; x < z; ++x) line(x, out);
+    });
+    for (int i = w0; i < w1 && ok; ++i) {
+      ok = std::fwrite(bufs[i].data(), 1, bufs[i].size(), f) == bufs[i].size();
+      std::string().swap(bufs[i]);
+    }
+  }
+  return (std::fclose(f) == 0) && ok;
+}
+
+}  // namespace mospb200
+
+using mospb200::writeLinesParallel;
 
 bool runConcurrently(const std::vector<std::function<bool()>> &jobs) {
   std::vector<char> ok(jobs.size(), 0);
@@ -362,29 +526,44 @@ bool readCsrGraph(const std::string &prefix, CsrGraph &graph) {
 }
 
 bool writeCsrGraph(const std::string &prefix, const CsrGraph &graph) {
-  Writer rows(prefix + "RowPtr.txt"), cols(prefix + "ColInd.txt"), vals(prefix + "Values.txt");
-  if (!rows.ok() || !cols.ok() || !vals.ok()) {
+  const int K = graph.numberOfObjectives;
+  bool okRows = false, okCols = false, okVals = false;
+  auto num = [](std::string &out, long long x) {
+    char d[24];
+    out.append(d, std::to_chars(d, d + sizeof(d), x).ptr);
+  };
+  runConcurrently({
+      [&] {
+        return okRows = writeLinesParallel(prefix + "RowPtr.txt", graph.rowPtr.size(),
+                                           [&](size_t i, std::string &out) {
+                                             num(out, graph.rowPtr[i]);
+                                             out.push_back('\n');
+                                           });
+      },
+      [&] {
+        return okCols = writeLinesParallel(prefix + "ColInd.txt", graph.colInd.size(),
+                                           [&](size_t i, std::string &out) {
+                                             num(out, graph.colInd[i]);
+                                             out.push_back('\n');
+                                           });
+      },
+      [&] {
+        return okVals = writeLinesParallel(
+                   prefix + "Values.txt", static_cast<size_t>(graph.numberOfEdges()),
+                   [&](size_t e, std::string &out) {
+                     for (int k = 0; k < K; ++k) {
+                       num(out, graph.weight(static_cast<int>(e), k));
+                       if (k + 1 < K) out.push_back(' ');
+                     }
+                     out.push_back('\n');
+                   });
+      },
+  });
+  if (!okRows || !okCols || !okVals) {
     std::cout << "Error: Could not write CSR files: " << prefix << "\n";
     return false;
   }
-  for (int x : graph.rowPtr) {
-    rows.num(x);
-    rows.ch('\n');
-  }
-  for (int x : graph.colInd) {
-    cols.num(x);
-    cols.ch('\n');
-  }
-  const int K = graph.numberOfObjectives;
-  for (int e = 0; e < graph.numberOfEdges(); ++e) {
-    for (int k = 0; k < K; ++k) {
-      vals.num(graph.weight(e, k));
-      if (k + 1 < K) vals.ch(' ');
-    }
-    vals.ch('\n');
-  }
-  const bool a = rows.close(), b = cols.close(), c = vals.close();
-  return a && b && c;
+  return true;
 }
 
 bool saveCsrGraphBinary(const std::string &path, const CsrGraph &graph,
@@ -709,6 +888,60 @@ void transposeCsrGraph(const CsrGraph &graph, CsrGraph &reverse) {
   }
 }
 
+namespace {
+
+/// Chunked parse of "v x" lines (x an integer, or INF when allowInf): calls
+/// store(v, x) for every line (lines of a chunk in order, chunks in
+/// parallel, so store must tolerate concurrent calls for distinct v) and
+/// returns the number of lines; on the first bad line in file order prints
+/// the message of `errorOf(kind)` and returns -1.
+template <typename Store>
+long long parseVertexLines(const std::string &text, const std::string &path, bool allowInf,
+                           long long minX, int numberOfNodes, const char *badLine,
+                           const char *badVertex, const char *badValue, Store store) {
+  const int parts = ioParts(text.size());
+  const std::vector<size_t> b = lineChunks(text, parts);
+  std::vector<long long> listed(parts, 0);
+  std::vector<size_t> errPos(parts, SIZE_MAX);
+  std::vector<const char *> errWhat(parts, nullptr);
+  parallelRun(parts, [&](int i) {
+    Cursor c(text, b[i], b[i + 1]);
+    auto fail = [&](const char *what) {
+      errPos[i] = c.offset();
+      errWhat[i] = what;
+    };
+    for (;;) {
+      c.space();
+      if (c.done()) break;
+      long long v = 0, x = 0;
+      if (!c.integer(v)) return fail(badLine);
+      c.blanks();
+      if (allowInf && c.literal("INF")) {
+        x = DISTANCE_INF;
+      } else if (!c.integer(x)) {
+        return fail(badLine);
+      }
+      if (v < 0 || v >= numberOfNodes || (!allowInf && (x < minX || x >= numberOfNodes))) {
+        return fail(badVertex);
+      }
+      if (allowInf && x < minX) return fail(badValue);
+      ++listed[i];
+      store(v, x);
+    }
+  });
+  long long total = 0;
+  for (int i = 0; i < parts; ++i) {
+    if (errPos[i] != SIZE_MAX) {
+      errorAt(errWhat[i], path, lineOf(text, errPos[i]));
+      return -1;
+    }
+    total += listed[i];
+  }
+  return total;
+}
+
+}  // namespace
+
 bool readDistances(const std::string &path, int numberOfNodes, std::vector<long long> &distances) {
   std::string text;
   if (!slurp(path, text)) {
@@ -716,26 +949,12 @@ bool readDistances(const std::string &path, int numberOfNodes, std::vector<long 
     return false;
   }
   distances.assign(numberOfNodes, -1);  // -1: not listed yet
-  long long listed = 0;
-  Cursor c(text);
-  for (;;) {
-    c.space();
-    if (c.done()) break;
-    long long v = 0, d = 0;
-    if (!c.integer(v)) return errorAt("Invalid line in distances file", path, c.line());
-    c.blanks();
-    if (c.literal("INF")) {
-      d = DISTANCE_INF;
-    } else if (!c.integer(d)) {
-      return errorAt("Invalid line in distances file", path, c.line());
-    }
-    if (v < 0 || v >= numberOfNodes) {
-      return errorAt("Vertex ID out of range in distances file", path, c.line());
-    }
-    if (d < 0) return errorAt("Negative distance", path, c.line());
-    ++listed;
-    distances[v] = d;
-  }
+  long long *d = distances.data();
+  const long long listed = parseVertexLines(
+      text, path, true, 0, numberOfNodes, "Invalid line in distances file",
+      "Vertex ID out of range in distances file", "Negative distance",
+      [d](long long v, long long x) { __atomic_store_n(d + v, x, __ATOMIC_RELAXED); });
+  if (listed < 0) return false;
   if (listed != numberOfNodes ||
       std::find(distances.begin(), distances.end(), -1LL) != distances.end()) {
     std::cout << "Error: " << path << " must list each of the " << numberOfNodes
@@ -752,21 +971,12 @@ bool readParents(const std::string &path, int numberOfNodes, std::vector<int> &p
     return false;
   }
   parent.assign(numberOfNodes, -2);  // -2: not listed yet
-  long long listed = 0;
-  Cursor c(text);
-  for (;;) {
-    c.space();
-    if (c.done()) break;
-    long long v = 0, p = 0;
-    if (!c.integer(v)) return errorAt("Invalid line in SSSP tree file", path, c.line());
-    c.blanks();
-    if (!c.integer(p)) return errorAt("Invalid line in SSSP tree file", path, c.line());
-    if (v < 0 || v >= numberOfNodes || p < -1 || p >= numberOfNodes) {
-      return errorAt("Vertex ID out of range in SSSP tree file", path, c.line());
-    }
-    ++listed;
-    parent[v] = static_cast<int>(p);
-  }
+  int *p = parent.data();
+  const long long listed = parseVertexLines(
+      text, path, false, -1, numberOfNodes, "Invalid line in SSSP tree file",
+      "Vertex ID out of range in SSSP tree file", "Vertex ID out of range in SSSP tree file",
+      [p](long long v, long long x) { __atomic_store_n(p + v, static_cast<int>(x), __ATOMIC_RELAXED); });
+  if (listed < 0) return false;
   if (listed != numberOfNodes || std::find(parent.begin(), parent.end(), -2) != parent.end()) {
     std::cout << "Error: " << path << " must list each of the " << numberOfNodes
               << " vertices exactly once (" << listed << " lines).\n";
@@ -776,35 +986,29 @@ bool readParents(const std::string &path, int numberOfNodes, std::vector<int> &p
 }
 
 bool writeDistances(const std::string &path, const std::vector<long long> &distances) {
-  Writer w(path);
-  if (!w.ok()) {
-    std::cout << "Error: Could not write distances file: " << path << "\n";
-    return false;
-  }
-  for (size_t v = 0; v < distances.size(); ++v) {
-    w.num(static_cast<long long>(v));
-    w.ch(' ');
+  const bool ok = writeLinesParallel(path, distances.size(), [&](size_t v, std::string &out) {
+    char d[24];
+    out.append(d, std::to_chars(d, d + sizeof(d), static_cast<long long>(v)).ptr);
+    out.push_back(' ');
     if (distances[v] >= DISTANCE_INF / 2) {
-      w.str("INF");
+      out.append("INF");
     } else {
-      w.num(distances[v]);
+      out.append(d, std::to_chars(d, d + sizeof(d), distances[v]).ptr);
     }
-    w.ch('\n');
-  }
-  return w.close();
+    out.push_back('\n');
+  });
+  if (!ok) std::cout << "Error: Could not write distances file: " << path << "\n";
+  return ok;
 }
 
 bool writeParents(const std::string &path, const std::vector<int> &parent) {
-  Writer w(path);
-  if (!w.ok()) {
-    std::cout << "Error: Could not write SSSP tree file: " << path << "\n";
-    return false;
-  }
-  for (size_t v = 0; v < parent.size(); ++v) {
-    w.num(static_cast<long long>(v));
-    w.ch(' ');
-    w.num(parent[v]);
-    w.ch('\n');
-  }
-  return w.close();
+  const bool ok = writeLinesParallel(path, parent.size(), [&](size_t v, std::string &out) {
+    char d[24];
+    out.append(d, std::to_chars(d, d + sizeof(d), static_cast<long long>(v)).ptr);
+    out.push_back(' ');
+    out.append(d, std::to_chars(d, d + sizeof(d), parent[v]).ptr);
+    out.push_back('\n');
+  });
+  if (!ok) std::cout << "Error: Could not write SSSP tree file: " << path << "\n";
+  return ok;
 }

@@ -2,12 +2,19 @@
 // and the C ABI of this library (not installed).
 #pragma once
 
+#include <functional>
 #include <string>
 #include <vector>
 
 #include "csrGraph.cuh"
 
 namespace mospb200 {
+
+/// Writes `count` lines to path, formatting chunks of lines on all host
+/// cores (line(i, out) appends line i to out); the bytes equal a sequential
+/// writer's.
+bool writeLinesParallel(const std::string &path, size_t count,
+                        const std::function<void(size_t, std::string &)> &line);
 
 /// Sets the calling thread's last-error message of the C ABI
 /// (mosp_last_error) and returns `status` (defined with the C ABI).

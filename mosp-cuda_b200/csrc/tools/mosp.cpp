@@ -126,32 +126,21 @@ std::vector<T> slice(const std::vector<T> &all, int k, int n) {
 }
 
 bool writeCosts(const std::string &path, const std::vector<long long> &costs, int KG) {
-  FILE *f = std::fopen(path.c_str(), "w");
-  if (f == nullptr) return false;
   const size_t n = KG > 0 ? costs.size() / KG : 0;
-  std::string buf;
-  buf.reserve(1 << 22);
-  char d[24];
-  bool ok = true;
-  for (size_t v = 0; v < n; ++v) {
-    buf.append(d, std::to_chars(d, d + 24, v).ptr);
+  return mospb200::writeLinesParallel(path, n, [&](size_t v, std::string &out) {
+    char d[24];
+    out.append(d, std::to_chars(d, d + 24, v).ptr);
     for (int k = 0; k < KG; ++k) {
       const long long c = costs[v * KG + k];
-      buf.push_back(' ');
+      out.push_back(' ');
       if (c >= DISTANCE_INF / 2) {
-        buf.append("INF");
+        out.append("INF");
       } else {
-        buf.append(d, std::to_chars(d, d + 24, c).ptr);
+        out.append(d, std::to_chars(d, d + 24, c).ptr);
       }
     }
-    buf.push_back('\n');
-    if (buf.size() > (1u << 22)) {
-      ok = ok && std::fwrite(buf.data(), 1, buf.size(), f) == buf.size();
-      buf.clear();
-    }
-  }
-  ok = ok && std::fwrite(buf.data(), 1, buf.size(), f) == buf.size();
-  return std::fclose(f) == 0 && ok;
+    out.push_back('\n');
+  });
 }
 
 bool validate(const CsrGraph &updated, const MospResult &r, int source, const std::vector<int> &pref,
