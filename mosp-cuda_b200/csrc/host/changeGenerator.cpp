@@ -17,6 +17,7 @@
 #include <random>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <unordered_set>
 #include <utility>
 #include <vector>
@@ -171,12 +172,16 @@ bool generateChangeBatch(const CsrGraph &graph, const ChangeGeneratorOptions &op
 
   std::vector<std::vector<int>> trees;
   if (onTrees) {
+    // the K trees are independent: one thread each
+    trees.resize(K);
+    std::vector<std::thread> threads;
     for (int k = 0; k < K; ++k) {
-      std::vector<long long> dist;
-      std::vector<int> parent;
-      dijkstraCsrGraph(graph, k, opt.source, dist, parent);
-      trees.push_back(std::move(parent));
+      threads.emplace_back([&graph, &trees, &opt, k] {
+        std::vector<long long> dist;
+        dijkstraCsrGraph(graph, k, opt.source, dist, trees[k]);
+      });
     }
+    for (auto &t : threads) t.join();
   }
 
   std::vector<Edge> inserts;
@@ -192,26 +197,47 @@ bool generateChangeBatch(const CsrGraph &graph, const ChangeGeneratorOptions &op
   // pair, no self-loops
   std::vector<Edge> deletes, reweights;
   if (nDel > 0 || nRe > 0) {
+    // A pair (u,v) can repeat only inside row u (all edges) or among the K
+    // parents of v (tree edges), so the first occurrences are found per row
+    // / per vertex, in parallel over vertex ranges, and concatenated in
+    // order: the pool equals a sequential scan with a global seen-set.
     std::vector<Edge> pool;
-    std::unordered_set<uint64_t> seen;
-    if (onTrees) {
-      for (int v = 0; v < n; ++v) {
-        if (!allowed(v)) continue;
-        for (const auto &t : trees) {
-          const int p = t[v];
-          if (p >= 0 && seen.insert(pairKey(p, v)).second) pool.push_back({p, v});
+    const int parts = static_cast<int>(std::max<long long>(
+        1, std::min<long long>(std::max(1u, std::thread::hardware_concurrency()),
+                               (static_cast<long long>(graph.numberOfEdges()) + n) >> 18)));
+    std::vector<std::vector<Edge>> pieces(parts);
+    std::vector<std::thread> threads;
+    for (int j = 0; j < parts; ++j) {
+      threads.emplace_back([&, j] {
+        const int lo = static_cast<int>(static_cast<long long>(n) * j / parts);
+        const int hi = static_cast<int>(static_cast<long long>(n) * (j + 1) / parts);
+        std::vector<Edge> &out = pieces[j];
+        if (onTrees) {
+          for (int v = lo; v < hi; ++v) {
+            if (!allowed(v)) continue;
+            for (int k = 0; k < K; ++k) {
+              const int p = trees[k][v];
+              bool first = p >= 0;
+              for (int q = 0; q < k && first; ++q) first = trees[q][v] != p;
+              if (first) out.push_back({p, v});
+            }
+          }
+        } else {
+          std::vector<int> stamp(n, -1);  // row that last listed v
+          for (int u = lo; u < hi; ++u) {
+            if (!allowed(u)) continue;
+            for (int e = graph.rowPtr[u]; e < graph.rowPtr[u + 1]; ++e) {
+              const int v = graph.colInd[e];
+              if (u == v || !allowed(v) || stamp[v] == u) continue;
+              stamp[v] = u;
+              out.push_back({u, v});
+            }
+          }
         }
-      }
-    } else {
-      for (int u = 0; u < n; ++u) {
-        if (!allowed(u)) continue;
-        for (int e = graph.rowPtr[u]; e < graph.rowPtr[u + 1]; ++e) {
-          const int v = graph.colInd[e];
-          if (u == v || !allowed(v)) continue;
-          if (seen.insert(pairKey(u, v)).second) pool.push_back({u, v});
-        }
-      }
+      });
     }
+    for (auto &t : threads) t.join();
+    for (auto &piece : pieces) pool.insert(pool.end(), piece.begin(), piece.end());
     if (pool.empty()) {
       std::cout << "Error: No existing edges available for the batch.\n";
       return false;
