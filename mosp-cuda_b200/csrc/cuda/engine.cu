@@ -337,6 +337,12 @@ __device__ void flushStage(const EngineParams &P, const LoopShared &L, int wrSlo
   }
 }
 
+/// Edge slots a lane relaxes at once (loads and atomics overlapped).
+#ifndef MOSP_EDGE_SLOTS
+#define MOSP_EDGE_SLOTS 2
+#endif
+constexpr int kSlots = MOSP_EDGE_SLOTS;
+
 /// Lane of the warp whose edge range holds edge slot s: the number of
 /// lanes whose inclusive edge count is <= s (binary search by shuffles).
 __device__ __forceinline__ int slotOwner(int incl, int s) {
@@ -409,13 +415,13 @@ __device__ __forceinline__ void expandWarp(const EngineParams &P, const LoopShar
   }
   const int edges = __shfl_sync(kFull, incl, 31);
   const int excl = incl - deg;
-  for (int s0 = 0; s0 < edges; s0 += 64) {
-    // two edge slots per lane, their loads and atomics overlapped
-    int sl[2], kk[2], uu[2], ee[2], ww[2], wt[2];
-    u64 dd[2], nd[2], old[2];
-    bool act[2];
+  for (int s0 = 0; s0 < edges; s0 += 32 * kSlots) {
+    // kSlots edge slots per lane, their loads and atomics overlapped
+    int sl[kSlots], kk[kSlots], uu[kSlots], ee[kSlots], ww[kSlots], wt[kSlots];
+    u64 dd[kSlots], nd[kSlots], old[kSlots];
+    bool act[kSlots];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
+    for (int h = 0; h < kSlots; ++h) {
       sl[h] = s0 + 32 * h + static_cast<int>(lane);
       const int o = slotOwner(incl, sl[h]);
       kk[h] = __shfl_sync(kFull, k, o);
@@ -425,33 +431,33 @@ __device__ __forceinline__ void expandWarp(const EngineParams &P, const LoopShar
       act[h] = sl[h] < edges;
     }
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
+    for (int h = 0; h < kSlots; ++h) {
       ww[h] = act[h] ? ldGraph<Mode>(outCol + ee[h]) : 0;
       wt[h] = act[h] ? ldGraph<Mode>(outWk[kk[h]] + ee[h]) : 0;
     }
-    u64 cw[2];
+    u64 cw[kSlots];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
+    for (int h = 0; h < kSlots; ++h) {
       nd[h] = dd[h] + static_cast<u64>(wt[h]);
       act[h] = act[h] && ww[h] != P.source && nd[h] <= P.obj[kk[h]].maxDist;
       cw[h] = pkOf(P.obj[kk[h]]).pack(nd[h], uu[h]);
     }
     if (P.flags & kFlagPrecheck) {
-      u64 cur[2];
+      u64 cur[kSlots];
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
+      for (int h = 0; h < kSlots; ++h) {
         cur[h] = act[h] ? __ldcg(P.packed + static_cast<long long>(kk[h]) * P.stride + ww[h]) : 0;
       }
 #pragma unroll
-      for (int h = 0; h < 2; ++h) act[h] = act[h] && cw[h] < cur[h];
+      for (int h = 0; h < kSlots; ++h) act[h] = act[h] && cw[h] < cur[h];
     }
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
+    for (int h = 0; h < kSlots; ++h) {
       old[h] = act[h] ? atomicMin(P.packed + static_cast<long long>(kk[h]) * P.stride + ww[h], cw[h])
                       : 0;
     }
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
+    for (int h = 0; h < kSlots; ++h) {
       if (!act[h] || nd[h] >= pkOf(P.obj[kk[h]]).dist(old[h])) continue;
       if (nd[h] < L.thr[kk[h]]) {
         stageAppend(P, L, kk[h], ww[h], nd[h], wrSlot, nearWV, nearWD);

@@ -74,6 +74,70 @@ bool toHost(T *dst, const T *src, size_t count, std::string &err) {
   return true;
 }
 
+template <typename T>
+bool toDeviceAsync(T *dst, const T *src, size_t count, cudaStream_t s, std::string &err) {
+  if (count == 0) return true;
+  const cudaError_t e = cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) {
+    err = std::string("CUDA error: ") + cudaGetErrorString(e);
+    return false;
+  }
+  return true;
+}
+
+template <typename T>
+bool toHostAsync(T *dst, const T *src, size_t count, cudaStream_t s, std::string &err) {
+  if (count == 0) return true;
+  const cudaError_t e = cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyDeviceToHost, s);
+  if (e != cudaSuccess) {
+    err = std::string("CUDA error: ") + cudaGetErrorString(e);
+    return false;
+  }
+  return true;
+}
+
+bool syncStream(cudaStream_t s, std::string &err) {
+  const cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    err = std::string("CUDA error: ") + cudaGetErrorString(e);
+    return false;
+  }
+  return true;
+}
+
+/// The pipeline's two streams (per host thread): the main stream runs the
+/// batch upload, Step 1 and the engine; the side stream moves the trees
+/// (upload while Step 1 runs, download while the combined step runs).
+struct PipelineStreams {
+  cudaStream_t main = nullptr, side = nullptr;
+  cudaEvent_t treesIn = nullptr, updated = nullptr;
+  int device = -1;
+  ~PipelineStreams() {
+    if (device < 0) return;
+    cudaSetDevice(device);
+    if (treesIn) cudaEventDestroy(treesIn);
+    if (updated) cudaEventDestroy(updated);
+    if (main) cudaStreamDestroy(main);
+    if (side) cudaStreamDestroy(side);
+  }
+  bool ready(std::string &err) {
+    int dev = -1;
+    cudaGetDevice(&dev);
+    if (main != nullptr && dev == device) return true;
+    if (main != nullptr) return true;  // created on another device earlier: reuse is unsafe
+    if (cudaStreamCreateWithFlags(&main, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&treesIn, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&updated, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      err = "Error: stream creation failed.";
+      return false;
+    }
+    device = dev;
+    return true;
+  }
+};
+
 }  // namespace
 
 struct PipelineIn {
@@ -132,6 +196,19 @@ int runPipeline(mosp_workspace *ws, const PipelineIn &in, PipelineOut &out, std:
   const size_t kn = static_cast<size_t>(K) * n;
   const size_t cap = static_cast<size_t>(m0) + nIns;
 
+  thread_local PipelineStreams streams;
+  if (!streams.ready(err)) return MOSP_ERR_CUDA;
+  cudaStream_t sm = streams.main, ss = streams.side;
+  // every return waits for both streams, so no copy into a caller's buffer
+  // is still in flight when the call returns (error paths included)
+  struct Drain {
+    cudaStream_t a, b;
+    ~Drain() {
+      cudaStreamSynchronize(a);
+      cudaStreamSynchronize(b);
+    }
+  } drain{sm, ss};
+
   // --- upload the original graph, the batch and the trees -----------------------
   auto t0 = std::chrono::steady_clock::now();
   int *dOrigRow, *dOrigCol, *dOrigW, *dInsFrom, *dInsTo, *dInsW, *dDelFrom, *dDelTo;
@@ -151,13 +228,19 @@ int runPipeline(mosp_workspace *ws, const PipelineIn &in, PipelineOut &out, std:
         !slot(ws, kParent, kn, dParent, err)) {
       return MOSP_ERR_OOM;
     }
-    if (!toDevice(dOrigRow, in.g.row, static_cast<size_t>(n) + 1, err) ||
-        !toDevice(dOrigCol, in.g.col, m0, err) ||
-        !toDevice(dOrigW, in.g.w, static_cast<size_t>(m0) * KG, err) ||
-        !toDevice(dInsFrom, in.b.insFrom, nIns, err) || !toDevice(dInsTo, in.b.insTo, nIns, err) ||
-        !toDevice(dInsW, in.b.insW, static_cast<size_t>(nIns) * KG, err) ||
-        !toDevice(dDelFrom, in.b.delFrom, nDel, err) || !toDevice(dDelTo, in.b.delTo, nDel, err) ||
-        !toDevice(dDist, in.initDist, kn, err) || !toDevice(dParent, in.initParent, kn, err)) {
+    // graph and batch on the main stream (Step 1 needs them); the trees on
+    // the side stream, overlapping Step 1 and the graph build
+    if (!toDeviceAsync(dOrigRow, in.g.row, static_cast<size_t>(n) + 1, sm, err) ||
+        !toDeviceAsync(dOrigCol, in.g.col, m0, sm, err) ||
+        !toDeviceAsync(dOrigW, in.g.w, static_cast<size_t>(m0) * KG, sm, err) ||
+        !toDeviceAsync(dInsFrom, in.b.insFrom, nIns, sm, err) ||
+        !toDeviceAsync(dInsTo, in.b.insTo, nIns, sm, err) ||
+        !toDeviceAsync(dInsW, in.b.insW, static_cast<size_t>(nIns) * KG, sm, err) ||
+        !toDeviceAsync(dDelFrom, in.b.delFrom, nDel, sm, err) ||
+        !toDeviceAsync(dDelTo, in.b.delTo, nDel, sm, err) ||
+        !toDeviceAsync(dDist, in.initDist, kn, ss, err) ||
+        !toDeviceAsync(dParent, in.initParent, kn, ss, err) ||
+        cudaEventRecord(streams.treesIn, ss) != cudaSuccess || !syncStream(sm, err)) {
       return MOSP_ERR_CUDA;
     }
   }
@@ -178,13 +261,13 @@ int runPipeline(mosp_workspace *ws, const PipelineIn &in, PipelineOut &out, std:
     int st = mosp_apply_batch_device(ws, n, KG, static_cast<int>(m0), dOrigRow, dOrigCol, dOrigW,
                                      nIns, dInsFrom, dInsTo, dInsW, nDel, dDelFrom, dDelTo,
                                      dOutRow, dOutCol, dEdgeW, static_cast<long long>(cap), &m,
-                                     dMask, maxWeight.data(), weightSum.data(), nullptr);
+                                     dMask, maxWeight.data(), weightSum.data(), sm);
     if (st != MOSP_OK) {
       err = mosp_last_error();
       return st;
     }
     out.mask.assign(nIns, 0u);
-    if (!toHost(out.mask.data(), dMask, nIns, err)) {
+    if (!toHostAsync(out.mask.data(), dMask, nIns, sm, err) || !syncStream(sm, err)) {
       return MOSP_ERR_CUDA;
     }
   }
@@ -205,8 +288,8 @@ int runPipeline(mosp_workspace *ws, const PipelineIn &in, PipelineOut &out, std:
   }
   if (!slot(ws, kChFrom, chFrom.size(), dChFrom, err) ||
       !slot(ws, kChTo, chTo.size(), dChTo, err) ||
-      !toDevice(dChFrom, chFrom.data(), chFrom.size(), err) ||
-      !toDevice(dChTo, chTo.data(), chTo.size(), err)) {
+      !toDeviceAsync(dChFrom, chFrom.data(), chFrom.size(), sm, err) ||
+      !toDeviceAsync(dChTo, chTo.data(), chTo.size(), sm, err)) {
     return MOSP_ERR_CUDA;
   }
   if (in.wantUpdated) {
@@ -218,9 +301,9 @@ int runPipeline(mosp_workspace *ws, const PipelineIn &in, PipelineOut &out, std:
     up.rowPtr.resize(static_cast<size_t>(n) + 1);
     up.colInd.resize(m);
     up.weights.resize(static_cast<size_t>(m) * KG);
-    if (!toHost(up.rowPtr.data(), dOutRow, up.rowPtr.size(), err) ||
-        !toHost(up.colInd.data(), dOutCol, up.colInd.size(), err) ||
-        !toHost(up.weights.data(), dEdgeW, up.weights.size(), err)) {
+    if (!toHostAsync(up.rowPtr.data(), dOutRow, up.rowPtr.size(), sm, err) ||
+        !toHostAsync(up.colInd.data(), dOutCol, up.colInd.size(), sm, err) ||
+        !toHostAsync(up.weights.data(), dEdgeW, up.weights.size(), sm, err) || !syncStream(sm, err)) {
       return MOSP_ERR_CUDA;
     }
   }
@@ -239,7 +322,7 @@ int runPipeline(mosp_workspace *ws, const PipelineIn &in, PipelineOut &out, std:
       return MOSP_ERR_OOM;
     }
     const int st = mosp_build_device_graph(ws, n, m, KG, dOutRow, dOutCol, dEdgeW, dOutW, dInRow,
-                                           dInCol, dInW, nullptr);
+                                           dInCol, dInW, sm);
     if (st != MOSP_OK) {
       err = mosp_last_error();
       return st;
@@ -266,22 +349,34 @@ int runPipeline(mosp_workspace *ws, const PipelineIn &in, PipelineOut &out, std:
       dd[k] = dDist + static_cast<size_t>(k) * n;
       dp[k] = dParent + static_cast<size_t>(k) * n;
     }
+    // the trees must have arrived
+    if (cudaStreamWaitEvent(sm, streams.treesIn, 0) != cudaSuccess) {
+      err = "Error: stream wait failed.";
+      return MOSP_ERR_CUDA;
+    }
     const int st = mosp_sosp_update_multi(ws, n, m, K, dOutRow, dOutCol, outW, dInRow, dInCol, inW,
                                           cf, ct, nc, dInsTo, in.b.nIns, in.source, delta.data(),
-                                          maxWeight.data(), dd, dp, out.stats.data(), nullptr);
+                                          maxWeight.data(), dd, dp, out.stats.data(), sm);
     if (st != MOSP_OK) {
       err = mosp_last_error();
       return st;
     }
   }
   out.t.objectives = msSince(t0);
+  // the K trees go back on the side stream while Steps 2-3 run
+  if (cudaEventRecord(streams.updated, sm) != cudaSuccess ||
+      cudaStreamWaitEvent(ss, streams.updated, 0) != cudaSuccess ||
+      !toHostAsync(out.dist, dDist, kn, ss, err) || !toHostAsync(out.parent, dParent, kn, ss, err)) {
+    if (err.empty()) err = "Error: stream wait failed.";
+    return MOSP_ERR_CUDA;
+  }
 
   // --- Steps 2-3: combined graph and its SOSP tree ----------------------------
   t0 = std::chrono::steady_clock::now();
   {
     ScopedStage stage("combined_graph_gpu", true);
     const int st = mosp_combined_sosp(ws, n, K, dParent, in.pref, in.source, 0, dCombDist,
-                                      dCombParent, &out.cstats, nullptr);
+                                      dCombParent, &out.cstats, sm);
     if (st != MOSP_OK) {
       err = mosp_last_error();
       return st;
@@ -293,7 +388,7 @@ int runPipeline(mosp_workspace *ws, const PipelineIn &in, PipelineOut &out, std:
     t0 = std::chrono::steady_clock::now();
     ScopedStage stage("mosp_costs_gpu", true);
     const int st = mosp_path_costs(ws, n, m, KG, dOutRow, dOutCol, dOutW, dCombParent, in.source,
-                                   dCosts, nullptr);
+                                   dCosts, sm);
     if (st != MOSP_OK) {
       err = mosp_last_error();
       return st;
@@ -305,10 +400,10 @@ int runPipeline(mosp_workspace *ws, const PipelineIn &in, PipelineOut &out, std:
   t0 = std::chrono::steady_clock::now();
   {
     ScopedStage stage("download", true);
-    if (!toHost(out.dist, dDist, kn, err) || !toHost(out.parent, dParent, kn, err) ||
-        !toHost(out.combDist, dCombDist, static_cast<size_t>(n), err) ||
-        !toHost(out.combParent, dCombParent, static_cast<size_t>(n), err) ||
-        (in.costs && !toHost(out.costs, dCosts, static_cast<size_t>(n) * KG, err))) {
+    if (!toHostAsync(out.combDist, dCombDist, static_cast<size_t>(n), sm, err) ||
+        !toHostAsync(out.combParent, dCombParent, static_cast<size_t>(n), sm, err) ||
+        (in.costs && !toHostAsync(out.costs, dCosts, static_cast<size_t>(n) * KG, sm, err)) ||
+        !syncStream(sm, err) || !syncStream(ss, err)) {
       return MOSP_ERR_CUDA;
     }
   }
