@@ -583,9 +583,15 @@ __device__ bool nearFarLoop(const EngineParams &P, const int *outRow,
     int *nearWV = (it & 1) ? P.nearV0 : P.nearV1;
     u64 *nearWD = (it & 1) ? P.nearD0 : P.nearD1;
 
-    for (long long base = gwarp * 32; base < total; base += nwarps * 32) {
+    // items per warp: ceil(total / warps), between 8 and 32, so that an
+    // iteration is spread over every warp of the grid rather than over
+    // total / 32 of them (the edges of a warp's items still spread over
+    // all 32 lanes)
+    long long chunk = (total + nwarps - 1) / nwarps;
+    chunk = chunk < 8 ? 8 : (chunk > 32 ? 32 : chunk);
+    for (long long base = gwarp * chunk; base < total; base += nwarps * chunk) {
       const long long j = base + lane;
-      const bool valid = j < total;
+      const bool valid = static_cast<long long>(lane) < chunk && j < total;
       int k = 0;
       if (valid) {
         while (k + 1 < K && L.off[k + 1] <= j) ++k;
