@@ -134,6 +134,25 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def max_over_ranks(x, pg, device):
+    """The largest of every rank's x (every rank calls it in the same
+    order); x itself without a process group."""
+    if pg is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(units_per_rank, steps, local_total_ms, world, pg, device):
+    """Replicas: every rank processes units_per_rank per step; the job's
+    time is the slowest rank's. Returns (units/s of the whole job, that
+    time in ms)."""
+    total_ms = max_over_ranks(local_total_ms, pg, device)
+    return world * units_per_rank * steps / (total_ms / 1000.0), total_ms
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -243,14 +262,10 @@ def run_ours(args):
     clock = clocks.stop()
     phases = {"update": ws.last_phases(0), "combined": ws.last_phases(1),
               "update_loop": ws.loop_profile(0), "combined_loop": ws.loop_profile(1)}
-    total_ms = float(sum(step_ms))
+    value, total_ms = replica_throughput(changed, args.steps, float(sum(step_ms)), world, pg, "cuda")
     if pg:
-        t = torch.tensor([total_ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        total_ms = float(t.item())
         pg.barrier()
     ms_per_step = total_ms / args.steps
-    value = world * changed * args.steps / (total_ms / 1000.0)
 
     # roofline of the dominant kernel (the fused K-objective update)
     old_d, old_p = d0.cpu().numpy(), p0.cpu().numpy()
@@ -301,11 +316,7 @@ def run_ours(args):
             t0 = time.perf_counter()
             _, _, _, _, _, tm = host_ws.update_host(garr, barr, hd0, hp0, K, src, costs=True, out=outs)
             times.append(time.perf_counter() - t0)
-        e2e_s = float(np.mean(times))
-        if pg:
-            t = torch.tensor([e2e_s], device="cuda")
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            e2e_s = float(t.item())
+        e2e_s = max_over_ranks(float(np.mean(times)), pg, "cuda")
         m_upd = upd.m
         # original graph, batch, initial trees and the per-objective change
         # lists in; mask, K trees, the combined tree and the costs out
