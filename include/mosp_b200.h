@@ -155,6 +155,14 @@ int mosp_workspace_set_combined_delta(mosp_workspace *ws, long long delta);
 int mosp_workspace_set_local_rounds(mosp_workspace *ws, int update_rounds,
                                     int scratch_rounds);
 
+/* Narrow iterations: a near-far iteration with at most max_items items
+ * (default 512; 0 = never) runs on one CTA, which then expands what it
+ * produces for up to `rounds` CTA-local rounds (default 64) before the grid
+ * barrier - thin wavefronts of deep graphs and the tails of epochs then
+ * cost a CTA barrier per hop instead of a grid barrier. Results do not
+ * depend on it. No counterpart in the reference. */
+int mosp_workspace_set_narrow(mosp_workspace *ws, int max_items, int rounds);
+
 /* When on, mosp_update_device records its launch sequence (control-block
  * clears, the update and combined launches, the status readback) as one
  * CUDA graph and replays it while the launch parameters stay the same; it

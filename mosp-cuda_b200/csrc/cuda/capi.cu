@@ -103,6 +103,9 @@ struct mosp_workspace {
   // and from-scratch / combined-graph launches
   int roundsUpdate = 0;
   int roundsScratch = 2;
+  // narrow iterations (few items) run on one CTA with many local rounds
+  int narrowItems = 512;
+  int narrowRounds = 64;
   // CUDA graph of mosp_update_device's launch sequence (mosp_workspace_use_graphs)
   bool useGraphs = false;
   cudaStream_t captureStream = nullptr;
@@ -305,6 +308,8 @@ int checkRoot(mosp_workspace *ws, int source) {
 
 void fillLists(EngineParams &p, mosp_workspace *ws, int block) {
   p.localRounds = p.mode == kModeUpdate ? ws->roundsUpdate : ws->roundsScratch;
+  p.narrowItems = ws->narrowItems;
+  p.narrowRounds = ws->narrowRounds;
   p.sources = ws->nSources > 1 ? ws->sources : nullptr;
   p.nSources = ws->nSources > 1 ? ws->nSources : 0;
   p.flags = engineFlags();
@@ -714,6 +719,15 @@ int mosp_workspace_set_local_rounds(mosp_workspace *ws, int update_rounds, int s
   }
   ws->roundsUpdate = update_rounds;
   ws->roundsScratch = scratch_rounds;
+  return MOSP_OK;
+}
+
+int mosp_workspace_set_narrow(mosp_workspace *ws, int max_items, int rounds) {
+  if (ws == nullptr || max_items < 0 || rounds < 0 || rounds > 1024) {
+    return fail(MOSP_ERR_INVALID, "invalid narrow-iteration settings");
+  }
+  ws->narrowItems = max_items;
+  ws->narrowRounds = rounds;
   return MOSP_OK;
 }
 

@@ -587,9 +587,19 @@ __device__ bool nearFarLoop(const EngineParams &P, const int *outRow,
     // iteration is spread over every warp of the grid rather than over
     // total / 32 of them (the edges of a warp's items still spread over
     // all 32 lanes)
-    long long chunk = (total + nwarps - 1) / nwarps;
+    //
+    // A narrow iteration (at most P.narrowItems items, e.g. a deep graph's
+    // thin wavefront or the tail of an epoch) goes to CTA 0 alone, which
+    // then keeps expanding the entries it produces (up to P.narrowRounds
+    // CTA-local rounds, each a __syncthreads instead of a grid barrier)
+    // while the other CTAs go straight to the barrier.
+    const bool narrow = total <= P.narrowItems;
+    const long long myWarp = narrow ? warp : gwarp;
+    const long long allWarps = narrow ? static_cast<long long>(blockDim.x >> 5) : nwarps;
+    long long chunk = (total + allWarps - 1) / allWarps;
     chunk = chunk < 8 ? 8 : (chunk > 32 ? 32 : chunk);
-    for (long long base = gwarp * chunk; base < total; base += nwarps * chunk) {
+    const long long myEnd = (narrow && blockIdx.x != 0) ? 0 : total;
+    for (long long base = myWarp * chunk; base < myEnd; base += allWarps * chunk) {
       const long long j = base + lane;
       const bool valid = static_cast<long long>(lane) < chunk && j < total;
       int k = 0;
@@ -635,7 +645,8 @@ __device__ bool nearFarLoop(const EngineParams &P, const int *outRow,
     // entry expanded here is not flushed; the last round's appends are.
     // (Relaxations are monotone atomicMin, so expanding an entry earlier
     // than the next iteration would cannot change the fixed point.)
-    for (int r = 0; r < P.localRounds; ++r) {
+    const int rounds = narrow ? (blockIdx.x == 0 ? P.narrowRounds : 0) : P.localRounds;
+    for (int r = 0; r < rounds; ++r) {
       __syncthreads();
       if (threadIdx.x == 0) {
         int tot = 0;

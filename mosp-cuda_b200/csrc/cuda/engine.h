@@ -108,6 +108,8 @@ struct EngineParams {
   int nSources;
   int mode, maxRounds, nHeads, flags;
   int localRounds;  // CTA-local expansion rounds per near-far iteration (0: none)
+  int narrowItems;  // iterations with at most this many items run on CTA 0 alone
+  int narrowRounds; // CTA-local rounds of such an iteration
   long long timeoutNs;
   int *genPtr;                 // stamp generation, advanced by every launch
   const int *outRow, *outCol, *inRow, *inCol;

@@ -82,6 +82,7 @@ _SIGS = {
     "mosp_workspace_set_combined_delta": (_i, [_p, _ll]),
     "mosp_workspace_use_graphs": (_i, [_p, _i]),
     "mosp_workspace_set_local_rounds": (_i, [_p, _i, _i]),
+    "mosp_workspace_set_narrow": (_i, [_p, _i, _i]),
     "mosp_workspace_graph_launches": (_i, [_p, _ip]),
     "mosp_autotune_update": (_i, [_p, _i, _i, _i, _p, _p, _p, _p, _p, _p, _p, _p, _ip, _p, _i, _i,
                                   _llp, _llp, _ip, _p, _p, _p, _p, _llp, _llp, _ip, C.POINTER(C.c_float), _p]),
@@ -498,6 +499,9 @@ class Workspace:
 
     def set_local_rounds(self, update_rounds, scratch_rounds):
         check(lib().mosp_workspace_set_local_rounds(self._h, int(update_rounds), int(scratch_rounds)))
+
+    def set_narrow(self, max_items, rounds):
+        check(lib().mosp_workspace_set_narrow(self._h, int(max_items), int(rounds)))
 
     def use_graphs(self, on=True):
         check(lib().mosp_workspace_use_graphs(self._h, int(bool(on))))
