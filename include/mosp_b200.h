@@ -468,8 +468,9 @@ int mosp_debug_barrier_cost(mosp_workspace *ws, int rounds, int reads,
  * same trees as applying them one by one); a pass starts only when the memory it may
  * allocate fits in the free device memory minus `reserve_bytes` (unless no
  * pass is running). The persistent launches of different workers run one
- * at a time; their uploads, Step 1 kernels and downloads overlap. No
- * counterpart in the reference, which runs one update per invocation. */
+ * at a time (each fills the GPU); the workers' copies and host work overlap
+ * with them. No counterpart in the reference, which runs one update per
+ * invocation. */
 typedef struct mosp_server mosp_server;
 
 typedef struct mosp_server_result {
@@ -480,7 +481,8 @@ typedef struct mosp_server_result {
   int reserved;
   double queue_us;     /* submit -> pass start */
   double latency_us;   /* submit -> result in host memory */
-  unsigned long long checksum; /* FNV-1a of the combined distances, parents */
+  unsigned long long checksum; /* order-independent hash of the returned tree,
+                                  computed by mosp_server_wait */
 } mosp_server_result;
 
 typedef struct mosp_server_stats {

@@ -888,13 +888,16 @@ int mosp_apply_batch_device(mosp_workspace *ws, int n, int K, int m, const int *
   }
   const size_t need = applyScratchBytes(n, m, n_ins, n_del);
   if (need > ws->applyBytes) {
+    // grow by half again: batches of varying size then rarely reallocate
+    // (a reallocation's cudaFree waits for the whole device)
+    const size_t want = std::max(need, ws->applyBytes + ws->applyBytes / 2);
     if (ws->applyScratch) cudaFree(ws->applyScratch);
     ws->applyScratch = nullptr;
     ws->applyBytes = 0;
     unsigned char *p = nullptr;
-    if ((st = deviceAlloc(&p, need)) != MOSP_OK) return st;
+    if ((st = deviceAlloc(&p, want)) != MOSP_OK) return st;
     ws->applyScratch = p;
-    ws->applyBytes = need;
+    ws->applyBytes = want;
   }
   int sms = 0;
   MOSP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ws->device));

@@ -3,6 +3,8 @@
 #pragma once
 
 #include <functional>
+
+#include <cuda_runtime.h>
 #include <string>
 #include <vector>
 

@@ -23,8 +23,10 @@
 //   * overlap: the persistent cooperative launches (graph build, update,
 //     combined graph) each fill the GPU, and two of them must never share it
 //     (each waits at grid barriers for all of its CTAs), so they run one at a
-//     time under a lock; uploads, Step 1 kernels and result downloads of the
-//     other workers overlap with them.
+//     time under a lock. An engine launch holds every SM's register file,
+//     so other kernels (another worker's Step 1) wait for it too; what
+//     overlaps with it is the other workers' host work (merging batches,
+//     change lists, result handling) and their host<->device copies.
 // A response carries the graph's combined tree after the pass that included
 // the request and the version (number of batches applied to the graph) of
 // that state; equal versions give equal results however the batches were
@@ -60,7 +62,6 @@ double usBetween(Clock::time_point a, Clock::time_point b) {
 struct Result {
   std::vector<long long> combDist;
   std::vector<int> combParent;
-  unsigned long long checksum = 0;
 };
 
 struct Request {
@@ -129,12 +130,16 @@ struct Graph {
   }
 };
 
-/// A device array that grows on demand (contents are not kept).
+/// A device array that grows on demand, at least doubling (a reallocation's
+/// cudaFree waits for the whole device, so it should be rare); contents are
+/// not kept.
 template <typename T>
 struct Buf {
   T *p = nullptr;
   long long cap = 0;
-  int fit(long long need, std::string &err) { return grow(p, cap, need, err); }
+  int fit(long long need, std::string &err) {
+    return grow(p, cap, need <= cap ? need : std::max(need, 2 * cap), err);
+  }
   void release() {
     if (p) cudaFree(p);
     p = nullptr;
@@ -158,7 +163,7 @@ struct Staging {
   }
   int hostBytes(long long need, std::string &err) {
     if (need <= hostCap && host != nullptr) return MOSP_OK;
-    const long long want = need + need / 4 + 4096;
+    const long long want = std::max(need + need / 4, 2 * hostCap) + 4096;
     unsigned char *p = nullptr;
     if (cudaHostAlloc(reinterpret_cast<void **>(&p), static_cast<size_t>(want), 0) != cudaSuccess) {
       cudaGetLastError();
@@ -172,19 +177,23 @@ struct Staging {
   }
 };
 
-/// Checksum of a combined tree: FNV-1a style xor-multiply over 64-bit
-/// words (the distances, then the parents two at a time).
-unsigned long long checksumOf(const long long *d, const int *p, int n) {
-  unsigned long long h = 1469598103934665603ULL;
+unsigned long long mix64(unsigned long long x) {
+  x ^= x >> 31;
+  x *= 0x7fb5d329728ea185ULL;
+  x ^= x >> 27;
+  x *= 0x81dadef4bc2dd44dULL;
+  x ^= x >> 33;
+  return x;
+}
+
+/// Order-independent checksum of a tree: the sum over v of a mixed hash of
+/// (v, dist[v]) and of (v, parent[v]).
+unsigned long long checksumOf(const long long *dist, const int *parent, int n) {
+  unsigned long long h = 0;
   for (int v = 0; v < n; ++v) {
-    h ^= static_cast<unsigned long long>(d[v]);
-    h *= 1099511628211ULL;
-  }
-  for (int v = 0; v < n; v += 2) {
-    const unsigned long long lo = static_cast<unsigned>(p[v]);
-    const unsigned long long hi = v + 1 < n ? static_cast<unsigned>(p[v + 1]) : 0ULL;
-    h ^= lo | (hi << 32);
-    h *= 1099511628211ULL;
+    const unsigned long long key = static_cast<unsigned long long>(v) * 0x9e3779b97f4a7c15ULL;
+    h += mix64(key ^ static_cast<unsigned long long>(dist[v])) +
+         mix64(~key ^ static_cast<unsigned long long>(static_cast<unsigned>(parent[v])));
   }
   return h;
 }
@@ -480,7 +489,7 @@ int mosp_server::runPass(mosp_workspace *ws, cudaStream_t s, Staging &st, Graph 
   std::memcpy(res->combDist.data(), st.host, static_cast<size_t>(n) * 8);
   std::memcpy(res->combParent.data(), st.host + static_cast<size_t>(n) * 8,
               static_cast<size_t>(n) * 4);
-  res->checksum = checksumOf(res->combDist.data(), res->combParent.data(), n);
+  // (the checksum is computed by mosp_server_wait, in the client's thread)
   const Clock::time_point tDone = Clock::now();
   {
     std::lock_guard<std::mutex> lk(mu);
@@ -770,7 +779,8 @@ extern "C" int mosp_server_wait(mosp_server *s, long long ticket, long long *h_c
     info->reserved = 0;
     info->queue_us = usBetween(r->submit, r->start);
     info->latency_us = usBetween(r->submit, r->done);
-    info->checksum = r->result ? r->result->checksum : 0;
+    info->checksum =
+        r->result ? checksumOf(r->result->combDist.data(), r->result->combParent.data(), n) : 0;
   }
   if (r->status != MOSP_OK) return recordFailure(r->status, r->error.c_str());
   if (h_comb_dist) std::memcpy(h_comb_dist, r->result->combDist.data(), static_cast<size_t>(n) * 8);

@@ -222,8 +222,10 @@ class HostGraph:
         row, col, w = _ip(), _ip(), _ip()
         check(lib().mosp_graph_arrays(self._h, C.byref(row), C.byref(col), C.byref(w)))
         r = np.ctypeslib.as_array(row, (self.n + 1,)).copy()
-        c = np.ctypeslib.as_array(col, (max(self.m, 1),))[: self.m].copy()
-        ww = np.ctypeslib.as_array(w, (max(self.m * self.K, 1),))[: self.m * self.K].copy()
+        if self.m == 0:  # no edges: the column and weight arrays may be NULL
+            return r, np.zeros(0, np.int32), np.zeros((0, self.K), np.int32)
+        c = np.ctypeslib.as_array(col, (self.m,)).copy()
+        ww = np.ctypeslib.as_array(w, (self.m * self.K,)).copy()
         return r, c, ww.reshape(self.m, self.K)
 
     @classmethod
