@@ -20,7 +20,8 @@
  *   - multi-objective arrays are objective-major: x[k * n + v].
  *
  * Calls on one workspace must not overlap; a workspace is bound to the
- * device that was current when it was created.
+ * device that was current when it was created, and every call that takes
+ * it makes that device current for the calling thread.
  */
 #ifndef MOSP_B200_H
 #define MOSP_B200_H

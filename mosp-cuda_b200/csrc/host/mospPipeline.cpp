@@ -112,19 +112,28 @@ struct PipelineStreams {
   cudaStream_t main = nullptr, side = nullptr;
   cudaEvent_t treesIn = nullptr, updated = nullptr;
   int device = -1;
-  ~PipelineStreams() {
+  ~PipelineStreams() { release(); }
+  void release() {
     if (device < 0) return;
+    int current = -1;
+    cudaGetDevice(&current);
     cudaSetDevice(device);
     if (treesIn) cudaEventDestroy(treesIn);
     if (updated) cudaEventDestroy(updated);
     if (main) cudaStreamDestroy(main);
     if (side) cudaStreamDestroy(side);
+    treesIn = updated = nullptr;
+    main = side = nullptr;
+    device = -1;
+    if (current >= 0) cudaSetDevice(current);
   }
+  /// Streams of the current device (recreated when the thread's device
+  /// changed since the last call).
   bool ready(std::string &err) {
     int dev = -1;
     cudaGetDevice(&dev);
     if (main != nullptr && dev == device) return true;
-    if (main != nullptr) return true;  // created on another device earlier: reuse is unsafe
+    release();
     if (cudaStreamCreateWithFlags(&main, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&treesIn, cudaEventDisableTiming) != cudaSuccess ||
@@ -196,6 +205,13 @@ int runPipeline(mosp_workspace *ws, const PipelineIn &in, PipelineOut &out, std:
   const size_t kn = static_cast<size_t>(K) * n;
   const size_t cap = static_cast<size_t>(m0) + nIns;
 
+  // make the workspace's device current (the workspace checks it on every
+  // call), then take this thread's streams of that device
+  int ctas = 0;
+  if (mosp_workspace_grid(ws, &ctas) != MOSP_OK) {
+    err = mosp_last_error();
+    return MOSP_ERR_CUDA;
+  }
   thread_local PipelineStreams streams;
   if (!streams.ready(err)) return MOSP_ERR_CUDA;
   cudaStream_t sm = streams.main, ss = streams.side;
