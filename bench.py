@@ -302,7 +302,11 @@ def run_ours(args):
     # end to end: host buffers through mosp_update_host
     e2e = None
     if args.e2e_steps > 0:
+        # the same widths and local rounds as the device-resident steps, set
+        # through the public API
         host_ws = mb.Workspace(timeout_ms=60000)
+        host_ws.set_combined_delta(comb_delta)
+        host_ws.set_local_rounds(*rounds)
         pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
         garr = tuple(pin(x) for x in (row, col, w))
         barr = {k: pin(v) for k, v in ba.items() if k != "mask"}
@@ -310,11 +314,13 @@ def run_ours(args):
         KG = w.shape[1]
         outs = (pin(np.empty(K * n, np.int64)), pin(np.empty(K * n, np.int32)), pin(np.empty(n, np.int64)),
                 pin(np.empty(n, np.int32)), pin(np.empty(n * KG, np.int64)))
-        host_ws.update_host(garr, barr, hd0, hp0, K, src, costs=True, out=outs)  # warm-up
+        e2e_delta = tuned[0] if len(set(tuned)) == 1 else 0  # one width for all objectives
+        host_ws.update_host(garr, barr, hd0, hp0, K, src, delta=e2e_delta, costs=True, out=outs)  # warm-up
         times = []
         for _ in range(args.e2e_steps):
             t0 = time.perf_counter()
-            _, _, _, _, _, tm = host_ws.update_host(garr, barr, hd0, hp0, K, src, costs=True, out=outs)
+            _, _, _, _, _, tm = host_ws.update_host(garr, barr, hd0, hp0, K, src, delta=e2e_delta, costs=True,
+                                                    out=outs)
             times.append(time.perf_counter() - t0)
         e2e_s = max_over_ranks(float(np.mean(times)), pg, "cuda")
         m_upd = upd.m

@@ -141,7 +141,8 @@ int mosp_workspace_set_sources(mosp_workspace *ws, const int *h_sources,
                                int count);
 
 /* Near-far bucket width of the combined-graph step run by
- * mosp_update_device (0 = the default heuristic of the reference,
+ * mosp_update_device, mosp_update_host and mosp_combined_sosp called with
+ * delta <= 0 (0 = the default heuristic of the reference,
  * src/combinedGraphGpu.cu:310-312). Results do not depend on it; the
  * autotuner (mosp_autotune_update) picks it. */
 int mosp_workspace_set_combined_delta(mosp_workspace *ws, long long delta);

@@ -1032,6 +1032,9 @@ int mosp_combined_sosp(mosp_workspace *ws, int n, int K, const int *d_parents, c
                        mosp_combine_stats *stats, void *stream) {
   int st = checkWorkspace(ws);
   if (st != MOSP_OK) return st;
+  // delta <= 0: the workspace's width (mosp_workspace_set_combined_delta),
+  // else the default heuristic
+  if (delta <= 0) delta = ws->combDelta;
   EngineParams p;
   long long scale = 0;
   int bits = 0;
