@@ -19,6 +19,12 @@ buffers (batch application, upload, GPU work, path costs and download inside
 the timed region).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload road|powerlaw|batched|serving]
+
+`--workload powerlaw` runs the same measurement on the power-law update
+(R-MAT scale 22, edge factor 16, K = 5, log-uniform weights in [1, 10^6],
+Pref = (1..5), 100,000 changes aimed at tree edges): the distance-only
+fallback with lowest-id parent recovery.
 
 Under torchrun every rank runs the same workload on its own GPU (replicas:
 one update does not shard); value = all ranks' changed edges / the slowest
@@ -62,18 +68,30 @@ def parse():
     ap.add_argument("--verify", action="store_true", help="check the result against the oracle")
     ap.add_argument("--requests", type=int, default=400, help="serving workload: requests per arrival rate")
     ap.add_argument("--rates", default="50,200,1000", help="serving workload: Poisson arrival rates (1/s)")
-    ap.add_argument("--workload", choices=["road", "batched", "serving"], default="road",
-                    help="road: the road-network update (default); batched: 256 grid-road instances in one "
-                         "launch against per-instance launches")
+    ap.add_argument("--workload", choices=["road", "powerlaw", "batched", "serving"], default="road",
+                    help="road: the road-network update (default); powerlaw: the R-MAT scale-22 update with the "
+                         "distance-only fallback; batched: 256 grid-road instances in one launch against "
+                         "per-instance launches; serving: the resident-graph request loop")
     ap.add_argument("--instances", type=int, default=256, help="batched workload: number of instances")
     return ap.parse_args()
 
 
+POWERLAW = ("power-law shape: R-MAT scale 22, edge factor 16, a=0.57 b=0.19 c=0.19, symmetrised, no self-loops "
+            "or duplicates; K=5 weights log-uniform in [1,1e6] seed 12345 (distance-only fallback with lowest-id "
+            "parent recovery); source 0; Pref=(1,2,3,4,5); 100,000 changes, 30% insertions, 70% deletions aimed "
+            "at tree edges (targeted mode, not connectivity-safe), seed 777")
+
+
 def make_workload(args):
+    """(graph, batch, K, Pref or None, description) of the workload."""
     import mosp_b200 as mb
+    if getattr(args, "workload", "road") == "powerlaw":
+        g = mb.HostGraph.rmat(22, 16, 0.57, 0.19, 0.19, 5, 1, 1_000_000, True, 12345)
+        batch = mb.HostBatch.generate(g, 100000, 30.0, "targeted", 0, False, 777, 0, 1, 1_000_000)
+        return g, batch, 5, [1, 2, 3, 4, 5], POWERLAW
     g = mb.HostGraph.grid_road(args.width, args.width, 0.70, 0.01, 3, 1, 100, 12345)
     batch = mb.HostBatch.generate(g, args.changes, 50.0, "uniform", 0, True, 777, 0, 1, 100)
-    return g, batch
+    return g, batch, 3, None, WORKLOAD
 
 
 def measured_peak():
@@ -176,8 +194,8 @@ def run_ours(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
         pg = dist
-    g, batch = make_workload(args)
-    K, n, src = 3, g.n, 0
+    g, batch, K, pref, workload = make_workload(args)
+    n, src = g.n, 0
     ws = mb.Workspace(timeout_ms=60000)
     ws.enable_timing(True)
     row, col, w = g.arrays()
@@ -188,7 +206,8 @@ def run_ours(args):
     maxw_orig = [int(w[:, k].max()) for k in range(K)]
     for k in range(K):
         ws.sosp_from_scratch(n, g.m, dg0.out_row, dg0.out_col, dg0.out_w_col(k), src,
-                             mb.default_delta(g.m, n, int(w[:, k].sum())), maxw_orig[k], d0[k], p0[k])
+                             mb.default_delta(g.m, n, int(w[:, k].astype(np.int64).sum())), maxw_orig[k],
+                             d0[k], p0[k])
     del dg0
     upd = mb.apply_batch(g, batch)
     ba = batch.arrays()
@@ -200,7 +219,8 @@ def run_ours(args):
     off = np.concatenate([[0], np.cumsum([len(c[0]) for c in ch])])
     heads = torch.from_numpy(ba["ins_to"]).cuda()
     maxw = [max(maxw_orig[k], int(ba["ins_w"][:, k].max())) for k in range(K)]
-    deltas = [args.delta if args.delta > 0 else mb.default_delta(g.m, n, int(w[:, k].sum())) for k in range(K)]
+    deltas = [args.delta if args.delta > 0 else mb.default_delta(g.m, n, int(w[:, k].astype(np.int64).sum()))
+              for k in range(K)]
     dist_t = torch.empty_like(d0)
     par_t = torch.empty_like(p0)
     cd = torch.empty(n, dtype=torch.int64, device="cuda")
@@ -216,7 +236,7 @@ def run_ours(args):
             s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             s.record(stream)
         stats, cst = ws.update_device(n, upd.m, K, dg.out_row, dg.out_col, dg.out_w, dg.in_row, dg.in_col, dg.in_w,
-                                      cf, ct, off, heads, len(ba["ins_to"]), src, widths, maxw, None, dist_t, par_t,
+                                      cf, ct, off, heads, len(ba["ins_to"]), src, widths, maxw, pref, dist_t, par_t,
                                       cd, cp, stream=None)
         if timed:
             e.record(stream)
@@ -235,7 +255,7 @@ def run_ours(args):
         par_t.copy_(p0)
         tuned, comb_delta, _, rounds = ws.autotune_update(n, upd.m, K, dg.out_row, dg.out_col, dg.out_w,
                                                           dg.in_row, dg.in_col, dg.in_w, cf, ct, off, heads,
-                                                          len(ba["ins_to"]), src, deltas, maxw, None, dist_t,
+                                                          len(ba["ins_to"]), src, deltas, maxw, pref, dist_t,
                                                           par_t, cd, cp)
         ws.set_combined_delta(comb_delta)
         ws.set_local_rounds(*rounds)
@@ -277,14 +297,14 @@ def run_ours(args):
     achieved = ab["update"] / (upd_mean / 1000.0) / 1e9
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tfile):
+    if os.path.exists(tfile) and workload == WORKLOAD:  # captured on the road workload
         try:
             traffic = json.load(open(tfile)).get("sosp_update_bytes_per_launch")
         except ValueError:
             traffic = None
     roofline = {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 5), "traffic": traffic,
-                "kernel": "sospEngine<update> (K=3 fused SOSP updates)",
+                "kernel": f"sospEngine<update> (K={K} fused SOSP updates)",
                 "algorithmic_bytes_per_launch": ab["update"], "kernel_ms": round(upd_mean, 4),
                 "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
                 else "fallback 6650 GB/s",
@@ -294,7 +314,7 @@ def run_ours(args):
     if args.verify:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle as orc
-        exp = orc.expected_update((row, col, w), ba, K, src)
+        exp = orc.expected_update((row, col, w), ba, K, src, pref)
         assert np.array_equal(new_d, exp["dist"]) and np.array_equal(new_p, exp["parent"])
         assert np.array_equal(cd.cpu().numpy(), exp["comb_dist"]) and np.array_equal(cp.cpu().numpy(),
                                                                                       exp["comb_parent"])
@@ -315,12 +335,13 @@ def run_ours(args):
         outs = (pin(np.empty(K * n, np.int64)), pin(np.empty(K * n, np.int32)), pin(np.empty(n, np.int64)),
                 pin(np.empty(n, np.int32)), pin(np.empty(n * KG, np.int64)))
         e2e_delta = tuned[0] if len(set(tuned)) == 1 else 0  # one width for all objectives
-        host_ws.update_host(garr, barr, hd0, hp0, K, src, delta=e2e_delta, costs=True, out=outs)  # warm-up
+        host_ws.update_host(garr, barr, hd0, hp0, K, src, pref=pref, delta=e2e_delta, costs=True,
+                            out=outs)  # warm-up
         times = []
         for _ in range(args.e2e_steps):
             t0 = time.perf_counter()
-            _, _, _, _, _, tm = host_ws.update_host(garr, barr, hd0, hp0, K, src, delta=e2e_delta, costs=True,
-                                                    out=outs)
+            _, _, _, _, _, tm = host_ws.update_host(garr, barr, hd0, hp0, K, src, pref=pref, delta=e2e_delta,
+                                                    costs=True, out=outs)
             times.append(time.perf_counter() - t0)
         e2e_s = max_over_ranks(float(np.mean(times)), pg, "cuda")
         m_upd = upd.m
@@ -338,13 +359,13 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_port(row, col, w, upd, ba, ch, old_d, old_p, K, src, changed)
+        cpu = cpu_baseline_port(row, col, w, upd, ba, ch, old_d, old_p, K, src, changed, pref)
 
     if rank == 0:
         line = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "n": n, "m": upd.m, "K": K, "changes_applied": changed,
+                "config": {"workload": workload, "n": n, "m": upd.m, "K": K, "changes_applied": changed,
                            "inserts": batch.n_ins, "deletes": batch.n_del, "parallelism": f"replicas x{world}",
                            "delta": tuned, "combined_delta": comb_delta or "default",
                            "local_rounds": {"update": rounds[0], "combined": rounds[1]},
@@ -366,7 +387,7 @@ def run_ours(args):
         pg.destroy_process_group()
 
 
-def cpu_baseline_port(row, col, w, upd, ba, ch, old_d, old_p, K, src, changed):
+def cpu_baseline_port(row, col, w, upd, ba, ch, old_d, old_p, K, src, changed, pref=None):
     """The oracle's restatement of the reference CPU path (sequential update
     per objective, then the host combined graph + Dijkstra), one full
     update, one thread."""
@@ -387,11 +408,11 @@ def cpu_baseline_port(row, col, w, upd, ba, ch, old_d, old_p, K, src, changed):
                                      orc.P(rcol), orc.P(rw), len(cf), orc.P(cf), orc.P(ct), len(heads),
                                      orc.P(heads), orc.P(d), orc.P(p))
         parents.append(p)
-    crow, ccol, cw = orc.combined_graph(np.stack(parents), len(urow) - 1, K, src, None)
+    crow, ccol, cw = orc.combined_graph(np.stack(parents), len(urow) - 1, K, src, pref)
     orc.dijkstra(crow, ccol, cw, 0, src)
     secs = time.perf_counter() - t0
     return {"value": round(changed / secs, 1), "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": "one full MOSP update of the workload (K=3 sequential SOSP updates + host combined graph "
+            "sample": f"one full MOSP update of the workload (K={K} sequential SOSP updates + host combined graph "
                       f"+ Dijkstra), compute only, {secs:.2f} s"}
 
 
@@ -728,8 +749,8 @@ def run_reference(args):
     import mosp_b200 as mb
     from concurrent.futures import ThreadPoolExecutor
 
-    g, batch = make_workload(args)
-    K, src = 3, 0
+    g, batch, K, pref, workload = make_workload(args)
+    src = 0
     row, col, w = g.arrays()
     ba = batch.arrays()
     changed = int(batch.n_ins + batch.n_del)
@@ -770,9 +791,9 @@ def run_reference(args):
             with ThreadPoolExecutor(max_workers=K) as pool:
                 parents = list(pool.map(objective, range(K)))
             if have_ref:
-                orc.ref_combined_dijkstra(np.stack(parents), g.n, K, src, None)
+                orc.ref_combined_dijkstra(np.stack(parents), g.n, K, src, pref)
             else:
-                crow, ccol, cw = orc.combined_graph(np.stack(parents), g.n, K, src, None)
+                crow, ccol, cw = orc.combined_graph(np.stack(parents), g.n, K, src, pref)
                 orc.dijkstra(crow, ccol, cw, 0, src)
             return time.perf_counter() - t0
 
@@ -784,14 +805,14 @@ def run_reference(args):
         value = changed / secs
         kind = "reference" if have_ref else "port"
         sample = (("reference sequentialSOSPUpdate (file API, text read/write included, as the reference's CPU "
-                   "path runs) per objective, K=3 objectives in parallel threads, then the reference "
+                   f"path runs) per objective, K={K} objectives in parallel threads, then the reference "
                    "combinedGraphReference + dijkstraCsrGraph") if have_ref else
                   "oracle restatement of the reference CPU path (compute only)")
         line = {"metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": steps,
                 "steps_requested": args.steps, "warmup": 1, "ms_per_step": round(secs * 1000, 2),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
                 "data": "synthetic", "impl": "reference",
-                "config": {"workload": WORKLOAD, "n": g.n, "m": upd.m, "K": K, "changes_applied": changed,
+                "config": {"workload": workload, "n": g.n, "m": upd.m, "K": K, "changes_applied": changed,
                            "parallelism": "CPU, one thread per objective"},
                 "cpu_baseline": {"value": round(value, 2), "unit": UNIT, "cores": K, "kind": kind,
                                  "sample": sample + f"; full workload per step, {steps} timed step(s)"},

@@ -768,50 +768,64 @@ __device__ bool unpackResults(const EngineParams &P, const int *outRow,
   }
   if (!anyFallback) return true;
   if (!gridSync(P.ctl, epoch)) return false;
+  // Lowest-id tight parent of every vertex of a distance-only objective:
+  // every edge (u, x) with d(u) + w = d(x) offers u to x by atomicMin, so
+  // the result does not depend on which thread checks which edge.
+  // Edge-balanced: warp w takes the w-th equal slice of the edge array and
+  // its lanes read 32 consecutive edges at a time (coalesced), so hub rows
+  // and hub-dense id ranges of power-law graphs cost no more than any other
+  // slice. The warp finds the source rows of its 32 edges from the ends of
+  // the next 32 rows (one coalesced load) by a 5-step shuffle search, and
+  // moves on 32 rows at a time through runs of empty rows.
   const unsigned lane = laneId();
   const long long gwarp = tid >> 5;
   const long long nwarps = T >> 5;
+  const long long m = ldGraph<Mode>(outRow + n);
   for (int k = 0; k < K; ++k) {
     const ObjectiveArgs &O = P.obj[k];
     if (O.parentBits > 0) continue;
     const long long ko = static_cast<long long>(k) * P.stride;
     const int *w = outWk[k];
-    for (long long base = gwarp * 32; base < n; base += nwarps * 32) {
-      const long long uu = base + lane;
-      int beg = 0, end = 0;
-      u64 du = kInfWord;
-      if (uu < n) {
-        du = __ldcg(P.packed + ko + uu);
-        if (du != kInfWord) {
-          beg = ldGraph<Mode>(outRow + uu);
-          end = ldGraph<Mode>(outRow + uu + 1);
+    const int wb = static_cast<int>(m * gwarp / nwarps);
+    const int we = static_cast<int>(m * (gwarp + 1) / nwarps);
+    if (wb >= we) continue;  // warp-uniform
+    // the row of the slice's first edge: the last r with rowPtr[r] <= wb
+    int lo = 0, hi = n;
+    while (hi - lo > 1) {
+      const int mid = lo + ((hi - lo) >> 1);
+      if (ldGraph<Mode>(outRow + mid) <= wb) lo = mid; else hi = mid;
+    }
+    int r0 = lo;  // no edge of the rest of the slice lies in a row before r0
+    for (int e0 = wb; e0 < we; e0 += 32) {
+      const int e = e0 + static_cast<int>(lane);
+      const bool live = e < we;
+      int row = live ? -1 : 0;
+      // at most ceil((n - r0) / 32) windows: the window holding row n - 1
+      // ends every search, since rows past n count as ending at INT_MAX
+      for (int base = r0; base < n; base += 32) {
+        const int rr = base + static_cast<int>(lane);
+        const int end = rr < n ? ldGraph<Mode>(outRow + rr + 1) : INT_MAX;
+        // pos = how many of the window's rows end at or before e
+        int pos = 0;
+#pragma unroll
+        for (int step = 16; step >= 1; step >>= 1) {
+          const int probe = __shfl_sync(kFull, end, pos + step - 1);
+          if (probe <= e) pos += step;
         }
+        const int lastEnd = __shfl_sync(kFull, end, 31);
+        if (row < 0 && e < lastEnd) row = base + pos;
+        if (__all_sync(kFull, row >= 0)) break;
       }
-      const int deg = end - beg;
-      unsigned big = __ballot_sync(kFull, deg > kLaneRowMax);
-      if (deg > 0 && deg <= kLaneRowMax) {
-        for (int e = beg; e < end; ++e) {
-          const int x = ldGraph<Mode>(outCol + e);
-          if (!isRoot(P.source, P.sources, P.nSources, x) &&
-              du + static_cast<u64>(ldGraph<Mode>(w + e)) == __ldcg(P.packed + ko + x)) {
-            atomicMin(O.parent + x, static_cast<int>(uu));
-          }
-        }
-      }
-      while (big != 0) {
-        const int src = __ffs(big) - 1;
-        big &= big - 1;
-        const int ub = static_cast<int>(__shfl_sync(kFull, uu, src));
-        const u64 db = __shfl_sync(kFull, du, src);
-        const int bb = __shfl_sync(kFull, beg, src);
-        const int eb = __shfl_sync(kFull, end, src);
-        for (int e = bb + static_cast<int>(lane); e < eb; e += 32) {
-          const int x = ldGraph<Mode>(outCol + e);
-          if (!isRoot(P.source, P.sources, P.nSources, x) &&
-              db + static_cast<u64>(ldGraph<Mode>(w + e)) == __ldcg(P.packed + ko + x)) {
-            atomicMin(O.parent + x, ub);
-          }
-        }
+      // lane 31 holds the largest row; when it is past the slice the loop
+      // ends here anyway
+      r0 = __shfl_sync(kFull, row, 31);
+      if (!live || row < 0) continue;
+      const u64 du = __ldcg(P.packed + ko + row);
+      if (du == kInfWord) continue;
+      const int x = ldGraph<Mode>(outCol + e);
+      if (!isRoot(P.source, P.sources, P.nSources, x) &&
+          du + static_cast<u64>(ldGraph<Mode>(w + e)) == __ldcg(P.packed + ko + x)) {
+        atomicMin(O.parent + x, row);
       }
     }
   }
