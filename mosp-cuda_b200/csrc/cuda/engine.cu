@@ -208,6 +208,13 @@ enum : int { kDone = 0, kPush = 1, kSplit = 2 };
 // path. Entries that do not fit the buffer take the direct global path.
 // ---------------------------------------------------------------------------
 constexpr int kStage = 8192;
+// Rows with more edges than this are expanded (push) or reduced (pull) by a
+// whole CTA instead of one warp: a power-law hub row (10^5 edges) would
+// otherwise keep one warp busy for the whole iteration. A launch turns
+// this on only when its graph has such rows (EngineControl::heavy, set in
+// the first phase), so graphs without them take no extra CTA barriers.
+constexpr int kHeavyDeg = 2048;
+constexpr int kHeavyCap = 64;
 
 struct StageHeader {
   int cap;                     // entries per list partition (kStage / (2K))
@@ -219,6 +226,15 @@ struct StageHeader {
   int base[2 * kMaxK];         // global start of this CTA's range
   u64 farMin[kMaxK];           // minimum distance appended to far (plain)
   long long expanded[kMaxK];   // non-stale expansions (statistics)
+  // heavy rows met by the CTA's warps, handled by the whole CTA afterwards
+  // (rows beyond kHeavyCap stay with their warp)
+  int heavyCount;
+  int heavyK[kHeavyCap];
+  int heavyU[kHeavyCap];
+  int heavyBeg[kHeavyCap];
+  int heavyDeg[kHeavyCap];
+  u64 heavyD[kHeavyCap];       // push: the row's distance; pull: the word before the pass
+  u64 heavyBest[kHeavyCap];    // pull: best word over the row, reduced by the CTA
 };
 
 struct StageEntry {
@@ -355,6 +371,54 @@ __device__ __forceinline__ int slotOwner(int incl, int s) {
   return lo;
 }
 
+/// Relaxation of edge e out of u (objective k, distance du): atomicMin of
+/// the word of its head, and the stage append of a strict improvement.
+template <int Mode>
+__device__ __forceinline__ void relaxEdge(const EngineParams &P, const LoopShared &L,
+                                          const int *outCol, const int *const *outWk, int k,
+                                          int u, u64 du, int e, int wrSlot, int *nearWV,
+                                          u64 *nearWD) {
+  const ObjectiveArgs &O = P.obj[k];
+  const Pk pk = pkOf(O);
+  const long long ko = static_cast<long long>(k) * P.stride;
+  const int w = ldGraph<Mode>(outCol + e);
+  const u64 nd = du + static_cast<u64>(ldGraph<Mode>(outWk[k] + e));
+  if (w == P.source || nd > O.maxDist) return;
+  const u64 old = atomicMin(P.packed + ko + w, pk.pack(nd, u));
+  if (nd >= pk.dist(old)) return;
+  if (nd < L.thr[k]) {
+    stageAppend(P, L, k, w, nd, wrSlot, nearWV, nearWD);
+  } else if (atomicExch(P.inFar + ko + w, 1) == 0) {
+    stageAppend(P, L, P.K + k, w, nd, wrSlot, nearWV, nearWD);
+  }
+}
+
+/// The CTA's queued heavy rows, each expanded by all threads of the CTA.
+/// Every thread of the CTA calls it; it starts with a barrier (so it also
+/// serves as the barrier after the expansion that queued the rows) and,
+/// when rows were queued, ends with one.
+template <int Mode>
+__device__ void expandHeavy(const EngineParams &P, const LoopShared &L, const int *outCol,
+                            const int *const *outWk, int wrSlot, int *nearWV, u64 *nearWD) {
+  StageHeader &H = stageHeader();
+  __syncthreads();
+  const int queued = H.heavyCount;
+  if (queued == 0) return;  // the same for every thread of the CTA
+  // every thread has read the count before it is reset; no warp queues a
+  // row again before the last barrier below
+  __syncthreads();
+  if (threadIdx.x == 0) H.heavyCount = 0;
+  const int count = queued < kHeavyCap ? queued : kHeavyCap;
+  for (int h = 0; h < count; ++h) {
+    const int k = H.heavyK[h], u = H.heavyU[h], beg = H.heavyBeg[h], end = beg + H.heavyDeg[h];
+    const u64 du = H.heavyD[h];
+    for (int e = beg + static_cast<int>(threadIdx.x); e < end; e += blockDim.x) {
+      relaxEdge<Mode>(P, L, outCol, outWk, k, u, du, e, wrSlot, nearWV, nearWD);
+    }
+  }
+  __syncthreads();
+}
+
 /// One warp expands up to 32 near entries, one per lane (u < 0: none):
 /// the edges of all lanes are spread over the warp, two slots per lane,
 /// with their loads and 64-bit atomicMin overlapped; every strict
@@ -364,7 +428,8 @@ template <int Mode>
 __device__ __forceinline__ void expandWarp(const EngineParams &P, const LoopShared &L,
                                            const int *outRow, const int *outCol,
                                            const int *const *outWk, int k, int u, u64 du, int beg,
-                                           int deg, int wrSlot, int *nearWV, u64 *nearWD) {
+                                           int deg, int wrSlot, int *nearWV, u64 *nearWD,
+                                           bool heavyOn) {
   StageHeader &H = stageHeader();
   const unsigned lane = laneId();
   const int K = P.K;
@@ -380,6 +445,19 @@ __device__ __forceinline__ void expandWarp(const EngineParams &P, const LoopShar
     }
   }
   if (__ballot_sync(kFull, deg > 0) == 0) return;
+  // heavy rows go to the CTA's queue (expanded by the whole CTA after this
+  // round of items) when the launch has any
+  if (heavyOn && deg > kHeavyDeg) {
+    const int slot = atomicAdd(&H.heavyCount, 1);
+    if (slot < kHeavyCap) {
+      H.heavyK[slot] = k;
+      H.heavyU[slot] = u;
+      H.heavyBeg[slot] = beg;
+      H.heavyDeg[slot] = deg;
+      H.heavyD[slot] = du;
+      deg = 0;
+    }
+  }
   // rows above 2^20 edges: whole-warp striding, one row at a time
   unsigned huge = __ballot_sync(kFull, deg > (1 << 20));
   while (huge != 0) {
@@ -502,6 +580,8 @@ __device__ bool nearFarLoop(const EngineParams &P, const int *outRow,
   }
 
   if (threadIdx.x < kMaxK) H.expanded[threadIdx.x] = 0;
+  // set before the grid barrier that precedes the loop, the same for all
+  const bool heavyOn = __ldcg(&c->heavy) != 0;
   int it = 0;
   unsigned long long profNs[2] = {0, 0};
   long long profIters[2] = {0, 0}, profItems[2] = {0, 0};
@@ -515,7 +595,10 @@ __device__ bool nearFarLoop(const EngineParams &P, const int *outRow,
       H.start[threadIdx.x] = 0;
     }
     if (threadIdx.x < kMaxK) H.farMin[threadIdx.x] = kInfWord;
-    if (threadIdx.x == 0) H.cap = kStage / (2 * K);
+    if (threadIdx.x == 0) {
+      H.cap = kStage / (2 * K);
+      H.heavyCount = 0;
+    }
     if (warp == 0) {
       const int k = static_cast<int>(lane);
       const bool act = k < K;
@@ -637,8 +720,10 @@ __device__ bool nearFarLoop(const EngineParams &P, const int *outRow,
         beg = ldGraph<Mode>(outRow + u);
         deg = ldGraph<Mode>(outRow + u + 1) - beg;
       }
-      expandWarp<Mode>(P, L, outRow, outCol, outWk, k, u, du, beg, deg, wrSlot, nearWV, nearWD);
+      expandWarp<Mode>(P, L, outRow, outCol, outWk, k, u, du, beg, deg, wrSlot, nearWV, nearWD,
+                       heavyOn);
     }
+    if (heavyOn) expandHeavy<Mode>(P, L, outCol, outWk, wrSlot, nearWV, nearWD);
     // Local rounds: the CTA expands the near entries it has just staged
     // itself, up to P.localRounds times while its partitions are at most
     // half full, so a frontier advances several hops per grid barrier. An
@@ -678,9 +763,14 @@ __device__ bool nearFarLoop(const EngineParams &P, const int *outRow,
           begq = ldGraph<Mode>(outRow + uq);
           degq = ldGraph<Mode>(outRow + uq + 1) - begq;
         }
-        expandWarp<Mode>(P, L, outRow, outCol, outWk, kq, uq, dq, begq, degq, wrSlot, nearWV, nearWD);
+        expandWarp<Mode>(P, L, outRow, outCol, outWk, kq, uq, dq, begq, degq, wrSlot, nearWV, nearWD,
+                         heavyOn);
       }
-      __syncthreads();
+      if (heavyOn) {
+        expandHeavy<Mode>(P, L, outCol, outWk, wrSlot, nearWV, nearWD);
+      } else {
+        __syncthreads();
+      }
       if (threadIdx.x < K) H.start[threadIdx.x] = H.roundEnd[threadIdx.x];
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) tWorked = globalNs();
@@ -960,6 +1050,13 @@ __global__ void __launch_bounds__(kThreads, 1) sospEngine(const __grid_constant_
 
   markPhase(c, kPhaseStart);
   if constexpr (Mode == kModeUpdate) {
+    // ---- Heavy rows: does the graph have rows for whole-CTA handling? -----
+    for (long long v = tid; v < n; v += T) {
+      if (__ldg(outRow + v + 1) - __ldg(outRow + v) > kHeavyDeg ||
+          __ldg(P.inRow + v + 1) - __ldg(P.inRow + v) > kHeavyDeg) {
+        c->heavy = 1;
+      }
+    }
     // ---- Pack the old trees; ancestors (reference :234-252) ---------------
     for (int k = 0; k < K; ++k) {
       const ObjectiveArgs &O = P.obj[k];
@@ -1121,9 +1218,14 @@ __global__ void __launch_bounds__(kThreads, 1) sospEngine(const __grid_constant_
         H.count[threadIdx.x] = 0;
         H.farMin[threadIdx.x] = kInfWord;
       }
-      if (threadIdx.x == 0) H.cap = kStage / K;
+      if (threadIdx.x == 0) {
+        H.cap = kStage / K;
+        H.heavyCount = 0;
+      }
       __syncthreads();
       const long long total = sOff[kMaxK];
+      // set in the first phase, the same for every thread of the grid
+      const bool heavyOn = __ldcg(&c->heavy) != 0;
       // Improved candidates go to far pile 0. With a partition of at least
       // one tile per objective (K * blockDim <= kStage) the appends are
       // staged per CTA and written out with one reservation per objective
@@ -1170,6 +1272,18 @@ __global__ void __launch_bounds__(kThreads, 1) sospEngine(const __grid_constant_
           cur = __ldcg(P.packed + ko + v);
           beg = __ldg(P.inRow + v);
           end = __ldg(P.inRow + v + 1);
+        }
+        // heavy in-rows are reduced by the whole CTA after the tile
+        if (heavyOn && end - beg > kHeavyDeg) {
+          const int slot = atomicAdd(&H.heavyCount, 1);
+          if (slot < kHeavyCap) {
+            H.heavyK[slot] = k;
+            H.heavyU[slot] = v;
+            H.heavyBeg[slot] = beg;
+            H.heavyDeg[slot] = end - beg;
+            H.heavyD[slot] = cur;
+            end = beg;
+          }
         }
         u64 best = cur;
         const int deg = end - beg;
@@ -1218,22 +1332,76 @@ __global__ void __launch_bounds__(kThreads, 1) sospEngine(const __grid_constant_
               const int idx = warpAppend(&c->farCount[k][0]);
               P.farL0[ko + idx] = v;
               warpMinInto(&c->farMinC[k][0], pk.dist(best));
-              continue;
-            }
-            const unsigned peers = __match_any_sync(__activemask(), k);
-            const int leader = __ffs(peers) - 1;
-            int rb = 0;
-            if (static_cast<int>(lane) == leader) rb = atomicAdd(&H.count[k], __popc(peers));
-            rb = __shfl_sync(peers, rb, leader);
-            E[k * H.cap + rb + __popc(peers & ((1u << lane) - 1u))].v = v;
-            const u64 d = pk.dist(best);
-            const unsigned hi = static_cast<unsigned>(d >> 32), lo = static_cast<unsigned>(d);
-            const unsigned mhi = __reduce_min_sync(peers, hi);
-            const unsigned mlo = __reduce_min_sync(peers, hi == mhi ? lo : 0xffffffffu);
-            if (static_cast<int>(lane) == leader) {
-              atomicMin(&H.farMin[k], (static_cast<u64>(mhi) << 32) | mlo);
+            } else {
+              const unsigned peers = __match_any_sync(__activemask(), k);
+              const int leader = __ffs(peers) - 1;
+              int rb = 0;
+              if (static_cast<int>(lane) == leader) rb = atomicAdd(&H.count[k], __popc(peers));
+              rb = __shfl_sync(peers, rb, leader);
+              E[k * H.cap + rb + __popc(peers & ((1u << lane) - 1u))].v = v;
+              const u64 d = pk.dist(best);
+              const unsigned hi = static_cast<unsigned>(d >> 32), lo = static_cast<unsigned>(d);
+              const unsigned mhi = __reduce_min_sync(peers, hi);
+              const unsigned mlo = __reduce_min_sync(peers, hi == mhi ? lo : 0xffffffffu);
+              if (static_cast<int>(lane) == leader) {
+                atomicMin(&H.farMin[k], (static_cast<u64>(mhi) << 32) | mlo);
+              }
             }
           }
+        }
+        if (heavyOn) {
+          // the tile's heavy in-rows: every thread of the CTA takes a share
+          // of each row, the partial minima meet in shared memory, and one
+          // thread per row writes the word and appends an improved vertex
+          // to the global far pile (as the unstaged path does)
+          __syncthreads();
+          const int queued = H.heavyCount;
+          if (queued > 0) {  // the same for every thread of the CTA
+            const int count = queued < kHeavyCap ? queued : kHeavyCap;
+            if (static_cast<int>(threadIdx.x) < count) H.heavyBest[threadIdx.x] = kInfWord;
+            __syncthreads();
+            if (threadIdx.x == 0) H.heavyCount = 0;
+            for (int h = 0; h < count; ++h) {
+              const int kh = H.heavyK[h], eh = H.heavyBeg[h] + H.heavyDeg[h];
+              const ObjectiveArgs &Oh = P.obj[kh];
+              const Pk ph = pkOf(Oh);
+              const long long koh = static_cast<long long>(kh) * P.stride;
+              u64 part = kInfWord;
+              for (int e = H.heavyBeg[h] + static_cast<int>(threadIdx.x); e < eh; e += blockDim.x) {
+                const int u = __ldg(P.inCol + e);
+                const u64 wd = __ldcg(P.packed + koh + u);
+                if (wd == kInfWord) continue;
+                const u64 nd = ph.dist(wd) + static_cast<u64>(__ldg(Oh.inW + e));
+                if (nd <= Oh.maxDist) {
+                  const u64 cw = ph.pack(nd, u);
+                  part = cw < part ? cw : part;
+                }
+              }
+              part = warpMinU64(part);
+              if (lane == 0 && part != kInfWord) atomicMin(&H.heavyBest[h], part);
+            }
+            __syncthreads();
+            if (static_cast<int>(threadIdx.x) < count) {
+              const int h = threadIdx.x;
+              const int kh = H.heavyK[h], vh = H.heavyU[h];
+              const Pk ph = pkOf(P.obj[kh]);
+              const long long koh = static_cast<long long>(kh) * P.stride;
+              const u64 curh = H.heavyD[h], besth = H.heavyBest[h];
+              if (besth < curh) {
+                // only this thread writes the word of vh during the pull pass
+                P.packed[koh + vh] = besth;
+                if (ph.dist(besth) < (curh == kInfWord ? kInfWord : ph.dist(curh))) {
+                  P.inFar[koh + vh] = 1;
+                  const int idx = atomicAdd(&c->farCount[kh][0], 1);
+                  P.farL0[koh + idx] = vh;
+                  atomicMax(&c->farMinC[kh][0], ~ph.dist(besth));
+                }
+              }
+            }
+          }
+          // every thread has read the queue (and the rows are done) before
+          // the next tile queues rows again
+          __syncthreads();
         }
         if (!staged) continue;
         // a tile appends at most blockDim entries: flush before a partition
@@ -1346,6 +1514,9 @@ __device__ void scratchOrCombined(const EngineParams &P, Sync &epoch, int genBas
   }
 
   // ---- SSSP from scratch: only the source (the roots) is finite ------------
+  for (long long v = tid; v < n; v += T) {
+    if (ldGraph<Mode>(outRow + v + 1) - ldGraph<Mode>(outRow + v) > kHeavyDeg) c->heavy = 1;
+  }
   for (int k = 0; k < K; ++k) {
     const Pk pk = pkOf(P.obj[k]);
     const long long ko = static_cast<long long>(k) * P.stride;

@@ -58,7 +58,8 @@ struct alignas(128) EngineControl {
   int rounds;            // pointer-jumping rounds
   int jumpActive[4];
   int finalGen;          // last stamp generation used
-  int pad2[3];
+  int heavy;             // the graph has rows of more than kHeavyDeg edges
+  int pad2[2];
   unsigned long long sums[2];  // combined graph: edges, weight sum
   int candCount[kMaxK];
   int invalidated[kMaxK];
