@@ -862,61 +862,76 @@ __device__ bool unpackResults(const EngineParams &P, const int *outRow,
   // every edge (u, x) with d(u) + w = d(x) offers u to x by atomicMin, so
   // the result does not depend on which thread checks which edge.
   // Edge-balanced: warp w takes the w-th equal slice of the edge array and
-  // its lanes read 32 consecutive edges at a time (coalesced), so hub rows
-  // and hub-dense id ranges of power-law graphs cost no more than any other
-  // slice. The warp finds the source rows of its 32 edges from the ends of
-  // the next 32 rows (one coalesced load) by a 5-step shuffle search, and
-  // moves on 32 rows at a time through runs of empty rows.
+  // its lanes read two windows of 32 consecutive edges at a time
+  // (coalesced), so hub rows and hub-dense id ranges of power-law graphs
+  // cost no more than any other slice. The warp finds the source rows of
+  // its edges from the ends of the next 32 rows (one coalesced load) by a
+  // 5-step shuffle search, moving on 32 rows at a time through runs of
+  // empty rows. The row search and the head loads are shared by all
+  // distance-only objectives, whose loads then go out together.
   const unsigned lane = laneId();
   const long long gwarp = tid >> 5;
   const long long nwarps = T >> 5;
   const long long m = ldGraph<Mode>(outRow + n);
-  for (int k = 0; k < K; ++k) {
-    const ObjectiveArgs &O = P.obj[k];
-    if (O.parentBits > 0) continue;
-    const long long ko = static_cast<long long>(k) * P.stride;
-    const int *w = outWk[k];
-    const int wb = static_cast<int>(m * gwarp / nwarps);
-    const int we = static_cast<int>(m * (gwarp + 1) / nwarps);
-    if (wb >= we) continue;  // warp-uniform
-    // the row of the slice's first edge: the last r with rowPtr[r] <= wb
-    int lo = 0, hi = n;
-    while (hi - lo > 1) {
-      const int mid = lo + ((hi - lo) >> 1);
-      if (ldGraph<Mode>(outRow + mid) <= wb) lo = mid; else hi = mid;
-    }
-    int r0 = lo;  // no edge of the rest of the slice lies in a row before r0
-    for (int e0 = wb; e0 < we; e0 += 32) {
-      const int e = e0 + static_cast<int>(lane);
-      const bool live = e < we;
-      int row = live ? -1 : 0;
-      // at most ceil((n - r0) / 32) windows: the window holding row n - 1
-      // ends every search, since rows past n count as ending at INT_MAX
-      for (int base = r0; base < n; base += 32) {
-        const int rr = base + static_cast<int>(lane);
-        const int end = rr < n ? ldGraph<Mode>(outRow + rr + 1) : INT_MAX;
-        // pos = how many of the window's rows end at or before e
-        int pos = 0;
+  const long long wb = m * gwarp / nwarps, we = m * (gwarp + 1) / nwarps;
+  if (wb >= we) return true;  // warp-uniform
+  // the row of the slice's first edge: the last r with rowPtr[r] <= wb
+  int lo = 0, hi = n;
+  while (hi - lo > 1) {
+    const int mid = lo + ((hi - lo) >> 1);
+    if (ldGraph<Mode>(outRow + mid) <= wb) lo = mid; else hi = mid;
+  }
+  int r0 = lo;  // no edge of the rest of the slice lies in a row before r0
+  for (long long e0 = wb; e0 < we; e0 += 64) {
+    const int ea = static_cast<int>(e0 + lane);
+    const int eb = static_cast<int>(e0 + 32 + lane);
+    const bool la = e0 + lane < we, lb = e0 + 32 + lane < we;
+    const int xa = la ? ldGraph<Mode>(outCol + ea) : 0;
+    const int xb = lb ? ldGraph<Mode>(outCol + eb) : 0;
+    int rowA = la ? -1 : 0, rowB = lb ? -1 : 0;
+    // at most ceil((n - r0) / 32) windows: the window holding row n - 1
+    // ends every search, since rows past n count as ending at INT_MAX
+    for (int base = r0; base < n; base += 32) {
+      const int rr = base + static_cast<int>(lane);
+      const int end = rr < n ? ldGraph<Mode>(outRow + rr + 1) : INT_MAX;
+      // pos = how many of the window's rows end at or before the edge
+      int posA = 0, posB = 0;
 #pragma unroll
-        for (int step = 16; step >= 1; step >>= 1) {
-          const int probe = __shfl_sync(kFull, end, pos + step - 1);
-          if (probe <= e) pos += step;
-        }
-        const int lastEnd = __shfl_sync(kFull, end, 31);
-        if (row < 0 && e < lastEnd) row = base + pos;
-        if (__all_sync(kFull, row >= 0)) break;
+      for (int step = 16; step >= 1; step >>= 1) {
+        const int probeA = __shfl_sync(kFull, end, posA + step - 1);
+        const int probeB = __shfl_sync(kFull, end, posB + step - 1);
+        if (probeA <= ea) posA += step;
+        if (probeB <= eb) posB += step;
       }
-      // lane 31 holds the largest row; when it is past the slice the loop
-      // ends here anyway
-      r0 = __shfl_sync(kFull, row, 31);
-      if (!live || row < 0) continue;
-      const u64 du = __ldcg(P.packed + ko + row);
-      if (du == kInfWord) continue;
-      const int x = ldGraph<Mode>(outCol + e);
-      if (!isRoot(P.source, P.sources, P.nSources, x) &&
-          du + static_cast<u64>(ldGraph<Mode>(w + e)) == __ldcg(P.packed + ko + x)) {
-        atomicMin(O.parent + x, row);
+      const int lastEnd = __shfl_sync(kFull, end, 31);
+      if (rowA < 0 && ea < lastEnd) rowA = base + posA;
+      if (rowB < 0 && eb < lastEnd) rowB = base + posB;
+      if (__all_sync(kFull, rowA >= 0 && rowB >= 0)) break;
+    }
+    // lane 31 of the second window holds the largest row; when it is past
+    // the slice the loop ends here anyway
+    r0 = __shfl_sync(kFull, rowB, 31);
+    const bool ca = la && rowA >= 0 && !isRoot(P.source, P.sources, P.nSources, xa);
+    const bool cb = lb && rowB >= 0 && !isRoot(P.source, P.sources, P.nSources, xb);
+    for (int k = 0; k < K; ++k) {
+      const ObjectiveArgs &O = P.obj[k];
+      if (O.parentBits > 0) continue;  // the same for every thread
+      const long long ko = static_cast<long long>(k) * P.stride;
+      const int *w = outWk[k];
+      u64 da = kInfWord, db = kInfWord, pa = 0, pb = 0;
+      int wa = 0, wbt = 0;
+      if (ca) {
+        da = __ldcg(P.packed + ko + rowA);
+        pa = __ldcg(P.packed + ko + xa);
+        wa = ldGraph<Mode>(w + ea);
       }
+      if (cb) {
+        db = __ldcg(P.packed + ko + rowB);
+        pb = __ldcg(P.packed + ko + xb);
+        wbt = ldGraph<Mode>(w + eb);
+      }
+      if (da != kInfWord && da + static_cast<u64>(wa) == pa) atomicMin(O.parent + xa, rowA);
+      if (db != kInfWord && db + static_cast<u64>(wbt) == pb) atomicMin(O.parent + xb, rowB);
     }
   }
   return true;
