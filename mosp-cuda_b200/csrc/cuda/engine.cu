@@ -93,36 +93,46 @@ __device__ __forceinline__ Sync startSync(long long timeoutNs) {
 /// Software grid barrier. Thread 0 of every CTA arrives on `arrive`; the
 /// last arrival publishes the epoch on `release`, which the others poll
 /// (acquire). The launch has one wall-clock deadline: a CTA that reaches a
-/// barrier after it, or waits past it, marks the run MOSP_ERR_TIMEOUT; the
-/// barrier then returns false in every CTA and the kernel must return. So a
-/// run ends by the deadline whether it stalls or keeps iterating.
+/// barrier after it marks the run MOSP_ERR_TIMEOUT and returns false
+/// without arriving, so the others cannot pass this barrier; a CTA that
+/// waits past it, or sees the status set while it waits (checked every 32
+/// polls, off the path of a release that arrives in time), does the same.
+/// A CTA that passed a barrier before the status was set returns false at
+/// the next one (the deadline has passed by then), and the kernel must
+/// return. So a run ends by the deadline whether it stalls or keeps
+/// iterating.
 __device__ bool gridSync(EngineControl *c, Sync &sync) {
   __shared__ int sOk;
   __syncthreads();
   if (threadIdx.x == 0) {
     const unsigned epoch = ++sync.epoch;
     int ok = 1;
-    if (globalNs() > sync.deadline) atomicCAS(&c->status, 0, MOSP_ERR_TIMEOUT);
-    __threadfence();
-    const unsigned prev = atomicAdd(&c->arrive, 1u);
-    if (prev + 1u == epoch * gridDim.x) {
-      stRelease(&c->release, epoch);
+    if (globalNs() > sync.deadline) {
+      atomicCAS(&c->status, 0, MOSP_ERR_TIMEOUT);
+      ok = 0;
     } else {
-      unsigned spin = 0;
-      while (static_cast<int>(ldAcquire(&c->release) - epoch) < 0) {
-        if (ldVolatile(&c->status) != 0) {
-          ok = 0;
-          break;
-        }
-        if ((++spin & 127u) == 0 && globalNs() > sync.deadline) {
-          atomicCAS(&c->status, 0, MOSP_ERR_TIMEOUT);
-          ok = 0;
-          break;
+      __threadfence();
+      const unsigned prev = atomicAdd(&c->arrive, 1u);
+      if (prev + 1u == epoch * gridDim.x) {
+        stRelease(&c->release, epoch);
+      } else {
+        unsigned spin = 0;
+        while (static_cast<int>(ldAcquire(&c->release) - epoch) < 0) {
+          if ((++spin & 31u) == 0) {
+            if (ldVolatile(&c->status) != 0) {
+              ok = 0;
+              break;
+            }
+            if (globalNs() > sync.deadline) {
+              atomicCAS(&c->status, 0, MOSP_ERR_TIMEOUT);
+              ok = 0;
+              break;
+            }
+          }
         }
       }
+      __threadfence();
     }
-    __threadfence();
-    if (ok && ldVolatile(&c->status) != 0) ok = 0;
     sOk = ok;
   }
   __syncthreads();
