@@ -73,6 +73,12 @@ def parse():
                          "distance-only fallback; batched: 256 grid-road instances in one launch against "
                          "per-instance launches; serving: the resident-graph request loop")
     ap.add_argument("--instances", type=int, default=256, help="batched workload: number of instances")
+    ap.add_argument("--rmat-scale", type=int, default=22,
+                    help="powerlaw workload: R-MAT scale (22 is the configuration; smaller sizes are for "
+                         "profiling captures)")
+    ap.add_argument("--rmat-wmax", type=int, default=1_000_000,
+                    help="powerlaw workload: largest weight (10^6 is the configuration; a smaller graph needs "
+                         "larger weights to take the distance-only fallback)")
     return ap.parse_args()
 
 
@@ -86,9 +92,14 @@ def make_workload(args):
     """(graph, batch, K, Pref or None, description) of the workload."""
     import mosp_b200 as mb
     if getattr(args, "workload", "road") == "powerlaw":
-        g = mb.HostGraph.rmat(22, 16, 0.57, 0.19, 0.19, 5, 1, 1_000_000, True, 12345)
-        batch = mb.HostBatch.generate(g, 100000, 30.0, "targeted", 0, False, 777, 0, 1, 1_000_000)
-        return g, batch, 5, [1, 2, 3, 4, 5], POWERLAW
+        scale = getattr(args, "rmat_scale", 22)
+        wmax = getattr(args, "rmat_wmax", 1_000_000)
+        g = mb.HostGraph.rmat(scale, 16, 0.57, 0.19, 0.19, 5, 1, wmax, True, 12345)
+        batch = mb.HostBatch.generate(g, 100000, 30.0, "targeted", 0, False, 777, 0, 1, wmax)
+        desc = POWERLAW
+        if scale != 22 or wmax != 1_000_000:
+            desc = desc.replace("R-MAT scale 22", f"R-MAT scale {scale}").replace("[1,1e6]", f"[1,{wmax}]")
+        return g, batch, 5, [1, 2, 3, 4, 5], desc
     g = mb.HostGraph.grid_road(args.width, args.width, 0.70, 0.01, 3, 1, 100, 12345)
     batch = mb.HostBatch.generate(g, args.changes, 50.0, "uniform", 0, True, 777, 0, 1, 100)
     return g, batch, 3, None, WORKLOAD

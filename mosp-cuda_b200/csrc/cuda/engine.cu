@@ -1053,6 +1053,38 @@ __device__ void scratchOrCombined(const EngineParams &P, Sync &epoch, int genBas
 // ---------------------------------------------------------------------------
 // The engine kernel
 // ---------------------------------------------------------------------------
+/// Pull pass: the best word that the in-edges e = first, first + step, ...
+/// (< end) offer to their head (objective with args O at offset ko), folded
+/// into `best`. Four edges per round with their loads in flight together
+/// (the column and weight loads, then the four tail words), so a long
+/// in-row is not one chain of dependent loads per edge.
+__device__ __forceinline__ u64 pullBest(const EngineParams &P, const ObjectiveArgs &O,
+                                        const Pk &pk, long long ko, int first, int end,
+                                        int step, u64 best) {
+  for (long long e0 = first; e0 < end; e0 += 4LL * step) {
+    int u[4], w[4];
+    u64 wd[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const long long e = e0 + static_cast<long long>(q) * step;
+      u[q] = e < end ? __ldg(P.inCol + e) : -1;
+      w[q] = e < end ? __ldg(O.inW + e) : 0;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) wd[q] = u[q] >= 0 ? __ldcg(P.packed + ko + u[q]) : kInfWord;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if (wd[q] == kInfWord) continue;
+      const u64 nd = pk.dist(wd[q]) + static_cast<u64>(w[q]);
+      if (nd <= O.maxDist) {
+        const u64 cw = pk.pack(nd, u[q]);
+        best = cw < best ? cw : best;
+      }
+    }
+  }
+  return best;
+}
+
 template <int Mode>
 __global__ void __launch_bounds__(kThreads, 1) sospEngine(const __grid_constant__ EngineParams P) {
   EngineControl *c = P.ctl;
@@ -1313,18 +1345,7 @@ __global__ void __launch_bounds__(kThreads, 1) sospEngine(const __grid_constant_
         u64 best = cur;
         const int deg = end - beg;
         unsigned big = __ballot_sync(kFull, deg > kLaneRowMax);
-        if (deg <= kLaneRowMax) {
-          for (int e = beg; e < end; ++e) {
-            const int u = __ldg(P.inCol + e);
-            const u64 wd = __ldcg(P.packed + ko + u);
-            if (wd == kInfWord) continue;
-            const u64 nd = pk.dist(wd) + static_cast<u64>(__ldg(O.inW + e));
-            if (nd <= O.maxDist) {
-              const u64 cw = pk.pack(nd, u);
-              best = cw < best ? cw : best;
-            }
-          }
-        }
+        if (deg <= kLaneRowMax) best = pullBest(P, O, pk, ko, beg, end, 1, best);
         while (big != 0) {
           const int src = __ffs(big) - 1;
           big &= big - 1;
@@ -1334,17 +1355,7 @@ __global__ void __launch_bounds__(kThreads, 1) sospEngine(const __grid_constant_
           const ObjectiveArgs &Ob = P.obj[kb];
           const Pk pb = pkOf(Ob);
           const long long kob = static_cast<long long>(kb) * P.stride;
-          u64 part = kInfWord;
-          for (int e = bb + static_cast<int>(lane); e < eb; e += 32) {
-            const int u = __ldg(P.inCol + e);
-            const u64 wd = __ldcg(P.packed + kob + u);
-            if (wd == kInfWord) continue;
-            const u64 nd = pb.dist(wd) + static_cast<u64>(__ldg(Ob.inW + e));
-            if (nd <= Ob.maxDist) {
-              const u64 cw = pb.pack(nd, u);
-              part = cw < part ? cw : part;
-            }
-          }
+          u64 part = pullBest(P, Ob, pb, kob, bb + static_cast<int>(lane), eb, 32, kInfWord);
           part = warpMinU64(part);
           if (static_cast<int>(lane) == src) best = part < best ? part : best;
         }
@@ -1391,17 +1402,8 @@ __global__ void __launch_bounds__(kThreads, 1) sospEngine(const __grid_constant_
               const ObjectiveArgs &Oh = P.obj[kh];
               const Pk ph = pkOf(Oh);
               const long long koh = static_cast<long long>(kh) * P.stride;
-              u64 part = kInfWord;
-              for (int e = H.heavyBeg[h] + static_cast<int>(threadIdx.x); e < eh; e += blockDim.x) {
-                const int u = __ldg(P.inCol + e);
-                const u64 wd = __ldcg(P.packed + koh + u);
-                if (wd == kInfWord) continue;
-                const u64 nd = ph.dist(wd) + static_cast<u64>(__ldg(Oh.inW + e));
-                if (nd <= Oh.maxDist) {
-                  const u64 cw = ph.pack(nd, u);
-                  part = cw < part ? cw : part;
-                }
-              }
+              u64 part = pullBest(P, Oh, ph, koh, H.heavyBeg[h] + static_cast<int>(threadIdx.x), eh,
+                                  static_cast<int>(blockDim.x), kInfWord);
               part = warpMinU64(part);
               if (lane == 0 && part != kInfWord) atomicMin(&H.heavyBest[h], part);
             }
