@@ -361,6 +361,14 @@ void readEvents(mosp_workspace *ws, float *first, float *second) {
 /// Queue one engine launch (control block `block` is cleared first).
 int queueEngine(mosp_workspace *ws, const EngineParams &p, int block, cudaStream_t s) {
   MOSP_CUDA(cudaMemsetAsync(ws->ctl + block, 0, sizeof(EngineControl), s));
+  if (needsHostRecovery(p)) {
+    // distance-only objectives: the parent recovery follows as its own kernel
+    EngineParams q = p;
+    q.flags |= kFlagHostRecovery;
+    MOSP_CUDA(launchEngine(q, ws->shape.engineCtas, s));
+    MOSP_CUDA(launchRecovery(q, s));
+    return MOSP_OK;
+  }
   MOSP_CUDA(launchEngine(p, ws->shape.engineCtas, s));
   return MOSP_OK;
 }
@@ -395,7 +403,14 @@ int launchUpdateGraph(mosp_workspace *ws, const EngineParams &pu, const EnginePa
     cudaStream_t c = ws->captureStream;
     MOSP_CUDA(cudaStreamBeginCapture(c, cudaStreamCaptureModeThreadLocal));
     cudaError_t err = cudaMemsetAsync(ws->ctl, 0, sizeof(EngineControl), c);
-    if (err == cudaSuccess) err = launchEngineEx(pu, ws->shape.engineCtas, c);
+    if (needsHostRecovery(pu)) {
+      EngineParams q = pu;
+      q.flags |= kFlagHostRecovery;
+      if (err == cudaSuccess) err = launchEngineEx(q, ws->shape.engineCtas, c);
+      if (err == cudaSuccess) err = launchRecovery(q, c);
+    } else if (err == cudaSuccess) {
+      err = launchEngineEx(pu, ws->shape.engineCtas, c);
+    }
     if (err == cudaSuccess) err = cudaMemsetAsync(ws->ctl + 1, 0, sizeof(EngineControl), c);
     if (err == cudaSuccess) err = launchEngineEx(pc, ws->shape.engineCtas, c);
     if (err == cudaSuccess) {

@@ -217,7 +217,10 @@ enum : int { kDone = 0, kPush = 1, kSplit = 2 };
 // CTA and list instead of one per warp group on the relaxation's critical
 // path. Entries that do not fit the buffer take the direct global path.
 // ---------------------------------------------------------------------------
-constexpr int kStage = 8192;
+#ifndef MOSP_STAGE_ENTRIES
+#define MOSP_STAGE_ENTRIES 8192
+#endif
+constexpr int kStage = MOSP_STAGE_ENTRIES;
 // Rows with more edges than this are expanded (push) or reduced (pull) by a
 // whole CTA instead of one warp: a power-law hub row (10^5 edges) would
 // otherwise keep one warp busy for the whole iteration. A launch turns
@@ -828,46 +831,13 @@ __device__ bool nearFarLoop(const EngineParams &P, const int *outRow,
   return true;
 }
 
-// ---------------------------------------------------------------------------
-// Unpack words into (distance, parent); distance-only objectives recover
-// the lowest-id tight parent (reference src/sospUpdateGpu.cu:478-512).
-// ---------------------------------------------------------------------------
+/// Lowest-id tight parent of every vertex of the distance-only objectives
+/// (parent INT_MAX after the unpack, -1 for roots and unreached vertices);
+/// thread tid of T.
 template <int Mode>
-__device__ bool unpackResults(const EngineParams &P, const int *outRow,
-                              const int *outCol, const int *const *outWk,
-                              Sync &epoch) {
+__device__ void recoverTightParents(const EngineParams &P, const int *outRow, const int *outCol,
+                                    const int *const *outWk, long long tid, long long T) {
   const int n = P.n, K = P.K;
-  const long long tid = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-  const long long T = static_cast<long long>(gridDim.x) * blockDim.x;
-  bool anyFallback = false;
-  for (int k = 0; k < K; ++k) {
-    const ObjectiveArgs &O = P.obj[k];
-    const Pk pk = pkOf(O);
-    const long long ko = static_cast<long long>(k) * P.stride;
-    if (O.parentBits > 0) {
-      for (long long v = tid; v < n; v += T) {
-        const u64 word = __ldcg(P.packed + ko + v);
-        if (word == kInfWord) {
-          O.dist[v] = kDistInf;
-          O.parent[v] = -1;
-        } else {
-          O.dist[v] = static_cast<long long>(pk.dist(word));
-          O.parent[v] = pk.parent(word);
-        }
-      }
-    } else {
-      anyFallback = true;
-      for (long long v = tid; v < n; v += T) {
-        const u64 word = __ldcg(P.packed + ko + v);
-        O.dist[v] = word == kInfWord ? kDistInf : static_cast<long long>(word);
-        O.parent[v] = (word == kInfWord || isRoot(P.source, P.sources, P.nSources, static_cast<int>(v)))
-                          ? -1
-                          : INT_MAX;
-      }
-    }
-  }
-  if (!anyFallback) return true;
-  if (!gridSync(P.ctl, epoch)) return false;
   // Lowest-id tight parent of every vertex of a distance-only objective:
   // every edge (u, x) with d(u) + w = d(x) offers u to x by atomicMin, so
   // the result does not depend on which thread checks which edge.
@@ -884,7 +854,7 @@ __device__ bool unpackResults(const EngineParams &P, const int *outRow,
   const long long nwarps = T >> 5;
   const long long m = ldGraph<Mode>(outRow + n);
   const long long wb = m * gwarp / nwarps, we = m * (gwarp + 1) / nwarps;
-  if (wb >= we) return true;  // warp-uniform
+  if (wb >= we) return;  // warp-uniform
   // the row of the slice's first edge: the last r with rowPtr[r] <= wb
   int lo = 0, hi = n;
   while (hi - lo > 1) {
@@ -944,6 +914,49 @@ __device__ bool unpackResults(const EngineParams &P, const int *outRow,
       if (db != kInfWord && db + static_cast<u64>(wbt) == pb) atomicMin(O.parent + xb, rowB);
     }
   }
+}
+
+// ---------------------------------------------------------------------------
+// Unpack words into (distance, parent); distance-only objectives recover
+// the lowest-id tight parent (reference src/sospUpdateGpu.cu:478-512).
+// ---------------------------------------------------------------------------
+template <int Mode>
+__device__ bool unpackResults(const EngineParams &P, const int *outRow,
+                              const int *outCol, const int *const *outWk,
+                              Sync &epoch) {
+  const int n = P.n, K = P.K;
+  const long long tid = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const long long T = static_cast<long long>(gridDim.x) * blockDim.x;
+  bool anyFallback = false;
+  for (int k = 0; k < K; ++k) {
+    const ObjectiveArgs &O = P.obj[k];
+    const Pk pk = pkOf(O);
+    const long long ko = static_cast<long long>(k) * P.stride;
+    if (O.parentBits > 0) {
+      for (long long v = tid; v < n; v += T) {
+        const u64 word = __ldcg(P.packed + ko + v);
+        if (word == kInfWord) {
+          O.dist[v] = kDistInf;
+          O.parent[v] = -1;
+        } else {
+          O.dist[v] = static_cast<long long>(pk.dist(word));
+          O.parent[v] = pk.parent(word);
+        }
+      }
+    } else {
+      anyFallback = true;
+      for (long long v = tid; v < n; v += T) {
+        const u64 word = __ldcg(P.packed + ko + v);
+        O.dist[v] = word == kInfWord ? kDistInf : static_cast<long long>(word);
+        O.parent[v] = (word == kInfWord || isRoot(P.source, P.sources, P.nSources, static_cast<int>(v)))
+                          ? -1
+                          : INT_MAX;
+      }
+    }
+  }
+  if (!anyFallback || (P.flags & kFlagHostRecovery) != 0) return true;
+  if (!gridSync(P.ctl, epoch)) return false;
+  recoverTightParents<Mode>(P, outRow, outCol, outWk, tid, T);
   return true;
 }
 
@@ -1786,6 +1799,21 @@ __global__ void barrierCost(EngineControl *c, int rounds, int reads, long long t
   if (blockIdx.x == 0 && threadIdx.x == 0) c->phaseNs[0] = globalNs() - t0;
 }
 
+/// The parent recovery of an update launch that ran with kFlagHostRecovery,
+/// as a kernel of its own: no shared-memory stage, so L1 keeps its full
+/// size for the graph reads.
+__global__ void __launch_bounds__(256) recoverParents(const __grid_constant__ EngineParams P) {
+  __shared__ const int *sOutWk[kMaxK];
+  if (threadIdx.x < kMaxK) {
+    sOutWk[threadIdx.x] =
+        static_cast<int>(threadIdx.x) < P.K ? P.obj[threadIdx.x].outW : nullptr;
+  }
+  __syncthreads();
+  const long long tid = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const long long T = static_cast<long long>(gridDim.x) * blockDim.x;
+  recoverTightParents<kModeUpdate>(P, P.outRow, P.outCol, sOutWk, tid, T);
+}
+
 template <typename Kernel>
 cudaError_t ctasFor(Kernel kernel, int sms, int ctasPerSm, int &ctas, size_t smem = 0) {
   int perSm = 0;
@@ -1833,6 +1861,23 @@ cudaError_t launchEngine(const EngineParams &p, int ctas, cudaStream_t s) {
     default: fn = reinterpret_cast<const void *>(sospEngine<kModeCombined>); break;
   }
   return cudaLaunchCooperativeKernel(fn, dim3(ctas), dim3(kThreads), args, kStageBytes, s);
+}
+
+bool needsHostRecovery(const EngineParams &p) {
+  if (p.mode != kModeUpdate) return false;
+  for (int k = 0; k < p.K; ++k) {
+    if (p.obj[k].parentBits == 0) return true;
+  }
+  return false;
+}
+
+cudaError_t launchRecovery(const EngineParams &p, cudaStream_t s) {
+  int device = 0, sms = 0;
+  cudaError_t err = cudaGetDevice(&device);
+  if (err == cudaSuccess) err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (err != cudaSuccess) return err;
+  recoverParents<<<sms * 8, 256, 0, s>>>(p);
+  return cudaGetLastError();
 }
 
 cudaError_t launchEngineEx(const EngineParams &p, int ctas, cudaStream_t s) {

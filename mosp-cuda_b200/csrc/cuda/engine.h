@@ -84,7 +84,9 @@ struct alignas(128) EngineControl {
 
 // EngineParams::flags (tuning switches; results do not depend on them)
 enum : int {
-  kFlagPrecheck = 1  // read the word before the atomicMin of a relaxation
+  kFlagPrecheck = 1,     // read the word before the atomicMin of a relaxation
+  kFlagHostRecovery = 2  // leave the lowest-id parent recovery of distance-only
+                         // objectives to recoverParents, launched right after
 };
 
 // Phase boundaries recorded in EngineControl::phaseNs.
@@ -170,6 +172,15 @@ cudaError_t launchEngine(const EngineParams &p, int ctas, cudaStream_t s);
 /// The same cooperative launch through cudaLaunchKernelEx with the
 /// cooperative attribute, the form a CUDA graph can capture.
 cudaError_t launchEngineEx(const EngineParams &p, int ctas, cudaStream_t s);
+
+/// An update launch with a distance-only objective: its parent recovery
+/// runs as a kernel of its own (all of L1 for the graph reads, where the
+/// update launch gives most of the SM's on-chip memory to its stage).
+bool needsHostRecovery(const EngineParams &p);
+
+/// The lowest-id tight parent recovery of the distance-only objectives of
+/// update launch `p` (which ran with kFlagHostRecovery), on stream s.
+cudaError_t launchRecovery(const EngineParams &p, cudaStream_t s);
 cudaError_t launchBuild(const BuildParams &p, int ctas, cudaStream_t s);
 cudaError_t launchCosts(const CostParams &p, int ctas, cudaStream_t s);
 cudaError_t launchBarrierProbe(EngineControl *ctl, long long timeoutNs,
