@@ -96,3 +96,21 @@ def test_fallback_with_hubs(ws):
     res = run_update_device(ws, g, b)
     assert all(s.packed_parents == 0 for s in res["stats"])
     assert_matches_oracle(res, g, b)
+
+
+def test_from_scratch_fallback_with_hubs(ws):
+    """SSSP from scratch with distance-only words: the lowest-id parent
+    recovery inside the launch (update launches run it as a kernel of its
+    own) on a graph with hub rows."""
+    n, W = 80000, 2_147_483_647
+    row, col, w = hub_graph(n, 100, 1, 1, W, 41)
+    assert mb.choose_packing(n, W)[0] == 0
+    g = mb.HostGraph.from_arrays(row, col, w)
+    dg = mb.DeviceGraph.upload(ws, g)
+    d = torch.empty(n, dtype=torch.int64, device="cuda")
+    p = torch.empty(n, dtype=torch.int32, device="cuda")
+    st = ws.sosp_from_scratch(n, g.m, dg.out_row, dg.out_col, dg.out_w, 0, 10 ** 12, W, d, p)
+    assert st.packed_parents == 0
+    de, pe = orc.dijkstra(row, col, w, 0, 0)
+    assert np.array_equal(d.cpu().numpy(), de)
+    assert np.array_equal(p.cpu().numpy(), pe)
