@@ -17,9 +17,17 @@
 //     MOSP_ERR_TIMEOUT instead of hanging the GPU;
 //   * subtree invalidation packs "ancestor or flag" into one int per
 //     vertex, so a pointer-jumping step is two dependent loads;
-//   * list appends are aggregated per warp and per destination list with
-//     __match_any_sync; rows longer than a warp are expanded by the whole
-//     warp, short rows one per lane.
+//   * list appends are staged per CTA in shared memory and written out
+//     with one reservation per list and iteration; a warp spreads the
+//     edges of its items over its lanes, and rows of more than 2,048 edges
+//     (power-law hubs) go to the whole CTA, in launches whose graph has
+//     them;
+//   * the pull pass scans in-rows four edges per round with their loads
+//     in flight together;
+//   * the lowest-id parent recovery of distance-only objectives is
+//     edge-balanced (equal edge slices per warp, a shuffle search for the
+//     rows) and, after an update launch, runs as its own kernel
+//     (recoverParents) so that L1 is not shared with the append stage.
 //
 // Result semantics (identical to the reference): words pack
 // (distance << b | parent) and only strictly better words are kept
