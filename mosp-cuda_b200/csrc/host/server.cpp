@@ -41,7 +41,6 @@
 #include <string>
 #include <thread>
 #include <unordered_map>
-#include <unordered_set>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -58,6 +57,71 @@ constexpr long long kPassChanges = 262144;  // changes per coalesced pass (after
 double usBetween(Clock::time_point a, Clock::time_point b) {
   return std::chrono::duration<double, std::micro>(b - a).count();
 }
+
+/// Set of (u, v) edge keys for the merge's conflict check: open addressing
+/// with linear probing in one flat array (no allocation per key; a pass can
+/// insert a few hundred thousand keys). Keys are u << 32 | v with u, v
+/// non-negative ints, so the all-ones word marks an empty slot.
+class EdgeKeySet {
+ public:
+  static unsigned long long key(int u, int v) {
+    return (static_cast<unsigned long long>(static_cast<unsigned>(u)) << 32) |
+           static_cast<unsigned>(v);
+  }
+  /// Empties the set, sized for `expected` keys at a load of at most 1/2.
+  void reset(size_t expected) {
+    size_t cap = 64;
+    while (cap < 2 * expected + 2) cap <<= 1;
+    if (slots_.size() == cap) {
+      std::fill(slots_.begin(), slots_.end(), kEmpty);
+    } else {
+      slots_.assign(cap, kEmpty);
+    }
+    count_ = 0;
+  }
+  bool empty() const { return count_ == 0; }
+  void insert(unsigned long long k) {
+    if (2 * (count_ + 1) > slots_.size()) rehash(2 * slots_.size());
+    size_t i = slot(k);
+    while (slots_[i] != kEmpty) {
+      if (slots_[i] == k) return;
+      i = (i + 1) & (slots_.size() - 1);
+    }
+    slots_[i] = k;
+    ++count_;
+  }
+  bool contains(unsigned long long k) const {
+    if (count_ == 0) return false;
+    size_t i = slot(k);
+    while (slots_[i] != kEmpty) {
+      if (slots_[i] == k) return true;
+      i = (i + 1) & (slots_.size() - 1);
+    }
+    return false;
+  }
+
+ private:
+  static constexpr unsigned long long kEmpty = ~0ULL;
+  size_t slot(unsigned long long k) const {
+    // 64-bit finaliser of MurmurHash3 (public domain), to spread the ids
+    k ^= k >> 33;
+    k *= 0xff51afd7ed558ccdULL;
+    k ^= k >> 33;
+    k *= 0xc4ceb9fe1a85ec53ULL;
+    k ^= k >> 33;
+    return static_cast<size_t>(k) & (slots_.size() - 1);
+  }
+  void rehash(size_t cap) {
+    std::vector<unsigned long long> old(cap, kEmpty);
+    old.swap(slots_);
+    count_ = 0;
+    for (unsigned long long k : old) {
+      if (k != kEmpty) insert(k);
+    }
+  }
+  std::vector<unsigned long long> slots_;
+  size_t count_ = 0;
+};
 
 struct Result {
   std::vector<long long> combDist;
@@ -301,19 +365,19 @@ int mosp_server::runPass(mosp_workspace *ws, cudaStream_t s, Staging &st, Graph 
   };
   std::vector<Merged> merges(1);
   {
-    std::unordered_set<unsigned long long> inserted;
-    auto key = [](int u, int v) {
-      return (static_cast<unsigned long long>(static_cast<unsigned>(u)) << 32) |
-             static_cast<unsigned>(v);
-    };
+    size_t groupInserts = 0;
+    for (auto &q : group) groupInserts += q->insFrom.size();
+    EdgeKeySet inserted;
+    inserted.reset(groupInserts);
+    auto key = EdgeKeySet::key;
     for (auto &q : group) {
       bool conflict = false;
       for (size_t i = 0; i < q->delFrom.size() && !conflict && !inserted.empty(); ++i) {
-        conflict = inserted.count(key(q->delFrom[i], q->delTo[i])) != 0;
+        conflict = inserted.contains(key(q->delFrom[i], q->delTo[i]));
       }
       if (conflict) {
         merges.emplace_back();
-        inserted.clear();
+        inserted.reset(groupInserts);
       }
       Merged &mg = merges.back();
       mg.insFrom.insert(mg.insFrom.end(), q->insFrom.begin(), q->insFrom.end());
