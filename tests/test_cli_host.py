@@ -103,6 +103,36 @@ def test_mosprep_byte_identical_to_reference(tmp_path):
         assert same_tree(ours / rel, ref / rel), str(rel)
 
 
+@pytest.mark.skipif(not os.path.exists(PREP_REF), reason="the reference's mospPrep was not built")
+def test_mosprep_multichunk_files_byte_identical(tmp_path):
+    """Files of several MB, which the readers and writers split into
+    line-aligned chunks parsed and formatted on all host cores: every file
+    equals the reference's sequential output byte for byte."""
+    rng = np.random.default_rng(5)
+    W = H = 400
+    u = np.arange(W * H).reshape(H, W) + 1
+    e = np.concatenate([np.stack([u[:, :-1].ravel(), u[:, 1:].ravel()], 1),
+                        np.stack([u[:-1, :].ravel(), u[1:, :].ravel()], 1)])
+    e = e[rng.random(len(e)) >= 0.05]
+    e = np.concatenate([e, e[:, ::-1]])
+    with open(tmp_path / "g.mtx", "w") as f:
+        f.write(f"%%MatrixMarket matrix coordinate pattern general\n{W * H} {W * H} {len(e)}\n")
+        f.write("\n".join(f"{a} {b}" for a, b in e) + "\n")
+    for tool, tag in ((PREP, "ours"), (PREP_REF, "ref")):
+        d = tmp_path / tag
+        run([tool, "mtx2csr", str(tmp_path / "g.mtx"), str(d / "csr/graphCsr"), "3", "1", "100", "5"], tmp_path)
+        run([tool, "init", str(d / "csr/graphCsr"), str(d / "init")], tmp_path)
+        run([tool, "changes", str(d / "csr/graphCsr"), str(d / "ch"), "--seed", "9", "--changes", "2000",
+             "--ins", "50"], tmp_path)
+        run([tool, "expected", str(d / "csr/graphCsr"), str(d / "ch"), str(d / "exp")], tmp_path)
+    ours, ref = tmp_path / "ours", tmp_path / "ref"
+    assert os.path.getsize(ref / "csr/graphCsrColInd.txt") > 3 << 20
+    files = [p.relative_to(ref) for p in ref.rglob("*.txt")]
+    assert len(files) >= 15
+    for rel in files:
+        assert same_tree(ours / rel, ref / rel), str(rel)
+
+
 def test_mosprep_init_matches_oracle(tmp_path):
     run([PREP, "grid", str(tmp_path / "g/graphCsr"), "25", "20", "0.8", "0.02", "2", "1", "50", "4"], tmp_path)
     run([PREP, "init", str(tmp_path / "g/graphCsr"), str(tmp_path / "init")], tmp_path)
