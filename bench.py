@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--changes", type=int, default=50000)
     ap.add_argument("--delta", type=int, default=0, help="fixed near-far width (0: default heuristic)")
     ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--loop", choices=["async", "bulk"], default="async",
+                    help="near-far loop of the persistent launches (results are the same)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--verify", action="store_true", help="check the result against the oracle")
     ap.add_argument("--requests", type=int, default=400, help="serving workload: requests per arrival rate")
@@ -209,6 +211,7 @@ def run_ours(args):
     n, src = g.n, 0
     ws = mb.Workspace(timeout_ms=60000)
     ws.enable_timing(True)
+    ws.set_async(args.loop == "async")
     row, col, w = g.arrays()
     # initial canonical trees of the original graph (GPU engine, from scratch)
     dg0 = mb.DeviceGraph.upload(ws, g)
@@ -337,6 +340,7 @@ def run_ours(args):
         # the same widths and local rounds as the device-resident steps, set
         # through the public API
         host_ws = mb.Workspace(timeout_ms=60000)
+        host_ws.set_async(args.loop == "async")
         host_ws.set_combined_delta(comb_delta)
         host_ws.set_local_rounds(*rounds)
         pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
@@ -384,6 +388,7 @@ def run_ours(args):
                            "delta_default": deltas,
                            "widths": "autotuned (mosp_autotune_update)" if args.delta <= 0 else "fixed by --delta",
                            "l2": "flushed (256 MiB write) before every timed step",
+                           "near_far_loop": args.loop,
                            "grid_ctas": ws.grid()},
                 "gpu_compute_ms": round(ms_per_step, 4),
                 "default_widths_ms_per_step": round(float(np.mean(default_ms)), 4),

@@ -165,6 +165,18 @@ int mosp_workspace_set_local_rounds(mosp_workspace *ws, int update_rounds,
  * depend on it. No counterpart in the reference. */
 int mosp_workspace_set_narrow(mosp_workspace *ws, int max_items, int rounds);
 
+/* Near-far loop of the persistent launches: on = 1 (default) runs it
+ * asynchronously - after each far-pile split every warp claims entries of
+ * a sharded near queue, expands them and pushes what improves, with no grid
+ * barrier until the phase has run dry - where the graph has no rows of more
+ * than 2,048 edges; 0 runs the bulk-synchronous loop (one grid barrier per
+ * iteration, the reference's schedule, src/sospUpdateGpu.cu:385-476) for
+ * every graph. queue_slots bounds the near queue (8 bytes a slot; 0 = one
+ * slot per vertex and objective plus n, at least 2^20): entries that find
+ * it full go to the far pile and are taken up in the next phase. Results
+ * do not depend on either. */
+int mosp_workspace_set_async(mosp_workspace *ws, int on, long long queue_slots);
+
 /* When on, mosp_update_device records its launch sequence (control-block
  * clears, the update and combined launches, the status readback) as one
  * CUDA graph and replays it while the launch parameters stay the same; it
@@ -317,13 +329,18 @@ int mosp_sosp_from_scratch(mosp_workspace *ws, int n, int m,
  * handlers, where an allocation may synchronize the device; plugin hosts
  * that forbid it). The engine's scratch is a file-scope __device__ array
  * reserved when the library's module is loaded, one per device; results
- * equal mosp_sosp_from_scratch's. No counterpart in the reference (whose
- * sospFromScratchGpu allocates, src/sospUpdateGpu.cu:719-745).
+ * equal mosp_sosp_from_scratch's. This entry point has no counterpart in
+ * the reference.
  *   - n <= MOSP_STATIC_MAX_VERTICES and m <= MOSP_STATIC_MAX_EDGES; larger
  *     graphs are rejected with MOSP_ERR_INVALID and a message.
+ *   - The CSR is checked on the device before it is used (row offsets
+ *     monotone from 0 to m, columns in [0, n)); a malformed graph returns
+ *     MOSP_ERR_INVALID.
  *   - Runs on the current device. The first call on a device does the
- *     setup (module load, symbol address, launch-shape query); make it
- *     before any stream capture on that device.
+ *     setup (module load, launch-shape query); make it before any stream
+ *     capture on that device. Every call looks up the array's device
+ *     address with that device current, so a device reset does not leave
+ *     a stale address behind.
  *   - The call clears the scratch regions that must start at zero (control
  *     block, stamp generation, stamps, in-far flags) in `stream` before the
  *     launch, so an aborted call leaves nothing behind.

@@ -66,7 +66,20 @@ struct mosp_workspace {
   int *nearV0 = nullptr, *nearV1 = nullptr;
   u64 *nearD0 = nullptr, *nearD1 = nullptr;
   int *gen = nullptr;  // device stamp generation
-  bool dirty = false;  // an aborted run may have left inFar/stamp set
+  bool dirty = false;  // an aborted run may have left inFar/stamp set (or queue slots filled)
+  // asynchronous near queue: aqCap slots (all ~0 between launches) in
+  // kAsyncShards shards, two counter sets
+  u64 *aqSlots = nullptr;
+  long long aqCap = 0;
+  AsyncShard *aqCtr = nullptr;
+  // near-far loop: 1 asynchronous where the graph allows it, 0 bulk
+  // (mosp_workspace_set_async); results do not depend on it
+  int asyncMode = 1;
+  long long asyncSlots = 0;  // queue size set by the caller (0: asyncSlotsFor)
+  // the last launch of each kind (0: update / scratch, 1: combined) found
+  // hub rows, so the next one goes straight to the bulk loop with its full
+  // stage
+  bool heavySeen[2] = {false, false};
   // control blocks
   EngineControl *ctl = nullptr;
   EngineControl *hostCtl = nullptr;  // pinned
@@ -142,6 +155,14 @@ void releaseNear(mosp_workspace *ws) {
   ws->nearK = 0;
 }
 
+void releaseAsync(mosp_workspace *ws) {
+  if (ws->aqSlots) cudaFree(ws->aqSlots);
+  if (ws->aqCtr) cudaFree(ws->aqCtr);
+  ws->aqSlots = nullptr;
+  ws->aqCtr = nullptr;
+  ws->aqCap = 0;
+}
+
 void releaseLists(mosp_workspace *ws) {
   for (void *p : {static_cast<void *>(ws->packed), static_cast<void *>(ws->val),
                   static_cast<void *>(ws->stamp), static_cast<void *>(ws->inFar),
@@ -155,6 +176,7 @@ void releaseLists(mosp_workspace *ws) {
   ws->nCap = 0;
   ws->kCap = 0;
   releaseNear(ws);
+  releaseAsync(ws);
 }
 
 int ensureShape(mosp_workspace *ws) {
@@ -195,6 +217,35 @@ int reserveNear(mosp_workspace *ws, long long n, long long m, int K) {
   return MOSP_OK;
 }
 
+/// Slots of the asynchronous near queue for K objectives of n vertices:
+/// one entry per vertex and objective plus n, at least 2^20 (or the size
+/// the caller set), in whole 32-slot claims per shard. A phase that pushes
+/// more moves the excess to the far piles, so this bounds memory, not
+/// correctness.
+long long asyncSlotsFor(long long n, int K, long long fixed = 0) {
+  const long long want = fixed > 0 ? fixed : std::max(n * K + n, 1LL << 20);
+  const long long perShard = (want + kAsyncShards - 1) / kAsyncShards;
+  return (perShard + 31) / 32 * 32 * kAsyncShards;
+}
+
+int reserveAsync(mosp_workspace *ws, long long n, int K) {
+  if (ws->asyncMode == 0) return MOSP_OK;
+  int st = MOSP_OK;
+  if (ws->aqCtr == nullptr) {
+    if ((st = deviceAlloc(&ws->aqCtr, 2 * kAsyncShards)) != MOSP_OK) return st;
+  }
+  const long long need = asyncSlotsFor(n, K, ws->asyncSlots);
+  if (need == ws->aqCap && ws->aqSlots != nullptr) return MOSP_OK;
+  if (ws->asyncSlots == 0 && need < ws->aqCap && ws->aqSlots != nullptr) return MOSP_OK;
+  if ((st = deviceAlloc(&ws->aqSlots, need)) != MOSP_OK) {
+    ws->aqCap = 0;
+    return st;
+  }
+  MOSP_CUDA(cudaMemset(ws->aqSlots, 0xff, need * sizeof(u64)));
+  ws->aqCap = need;
+  return MOSP_OK;
+}
+
 int reserveLists(mosp_workspace *ws, long long n, int K) {
   if (n <= ws->nCap && K <= ws->kCap) return MOSP_OK;
   const long long newN = std::max(n, ws->nCap);
@@ -226,6 +277,9 @@ int cleanLists(mosp_workspace *ws, cudaStream_t s) {
     MOSP_CUDA(cudaMemsetAsync(ws->inFar, 0, total * sizeof(int), s));
     MOSP_CUDA(cudaMemsetAsync(ws->stamp, 0, total * sizeof(int), s));
     MOSP_CUDA(cudaMemsetAsync(ws->gen, 0, sizeof(int), s));
+    if (ws->aqSlots != nullptr) {
+      MOSP_CUDA(cudaMemsetAsync(ws->aqSlots, 0xff, ws->aqCap * sizeof(u64), s));
+    }
     ws->dirty = false;
   }
   return MOSP_OK;
@@ -313,6 +367,22 @@ void fillLists(EngineParams &p, mosp_workspace *ws, int block) {
   p.sources = ws->nSources > 1 ? ws->sources : nullptr;
   p.nSources = ws->nSources > 1 ? ws->nSources : 0;
   p.flags = engineFlags();
+  // asynchronous loop unless it is off or the graph last seen here had hub
+  // rows; its launches need a smaller stage (the pull pass stays staged up
+  // to K tiles), which leaves more of the SM's memory to L1
+  const bool async = ws->asyncMode != 0 && ws->aqSlots != nullptr &&
+                     ws->aqCap >= asyncSlotsFor(p.n, p.K, ws->asyncSlots) &&
+                     !ws->heavySeen[block == 1 ? 1 : 0];
+  if (async) {
+    p.flags |= kFlagAsync;
+    p.aqSlots = ws->aqSlots;
+    p.aqCtr = ws->aqCtr;
+    p.aqShards = kAsyncShards;
+    p.aqShardCap = static_cast<unsigned>(ws->aqCap / kAsyncShards);
+    p.stageEntries = std::min(kStageEntriesMax, std::max(kStageEntriesAsync, p.K * kThreads));
+  } else {
+    p.stageEntries = kStageEntriesMax;
+  }
   p.timeoutNs = ws->timeoutNs;
   p.genPtr = ws->gen;
   p.packed = ws->packed;
@@ -503,6 +573,7 @@ int prepareUpdate(mosp_workspace *ws, const UpdateArgs &a, EngineParams &p, int 
   st = reserveLists(ws, a.n, a.K);
   if (st != MOSP_OK) return st;
   if ((st = reserveNear(ws, a.n, a.m, a.K)) != MOSP_OK) return st;
+  if ((st = reserveAsync(ws, a.n, a.K)) != MOSP_OK) return st;
   std::memset(&p, 0, sizeof(p));
   p.n = a.n;
   p.m = a.m;
@@ -557,6 +628,7 @@ int prepareCombined(mosp_workspace *ws, int n, int K, const int *d_parents, cons
   if (st != MOSP_OK) return st;
   if ((st = reserveCombined(ws, n, K)) != MOSP_OK) return st;
   if ((st = reserveNear(ws, n, static_cast<long long>(n) * K, 1)) != MOSP_OK) return st;
+  if ((st = reserveAsync(ws, n, 1)) != MOSP_OK) return st;
   std::memset(&p, 0, sizeof(p));
   p.n = n;
   p.K = 1;
@@ -743,6 +815,15 @@ int mosp_workspace_set_narrow(mosp_workspace *ws, int max_items, int rounds) {
   }
   ws->narrowItems = max_items;
   ws->narrowRounds = rounds;
+  return MOSP_OK;
+}
+
+int mosp_workspace_set_async(mosp_workspace *ws, int on, long long queue_slots) {
+  if (ws == nullptr || on < 0 || on > 1 || queue_slots < 0 || queue_slots > (1LL << 34)) {
+    return fail(MOSP_ERR_INVALID, "invalid near-far loop mode");
+  }
+  ws->asyncMode = on;
+  ws->asyncSlots = queue_slots;
   return MOSP_OK;
 }
 
@@ -982,6 +1063,7 @@ int mosp_sosp_update_multi(mosp_workspace *ws, int n, int m, int K, const int *d
   if ((st = readControl(ws, 0, 1, s)) != MOSP_OK) return st;
   readEvents(ws, &ws->lastUpdateMs, nullptr);
   const EngineControl &c = ws->hostCtl[0];
+  ws->heavySeen[0] = c.heavy != 0;
   if ((st = controlStatus(ws, c)) != MOSP_OK) return st;
   if (stats) {
     for (int k = 0; k < K; ++k) fillStats(c, k, bits[k], stats + k);
@@ -1015,6 +1097,7 @@ int mosp_sosp_from_scratch(mosp_workspace *ws, int n, int m, const int *d_out_ro
   if ((st = checkRoot(ws, source)) != MOSP_OK) return st;
   if ((st = reserveLists(ws, n, 1)) != MOSP_OK) return st;
   if ((st = reserveNear(ws, n, m, 1)) != MOSP_OK) return st;
+  if ((st = reserveAsync(ws, n, 1)) != MOSP_OK) return st;
   int bits = 0;
   u64 maxDist = 0;
   if ((st = choosePacking(n, max_weight, bits, maxDist)) != MOSP_OK) return st;
@@ -1037,6 +1120,7 @@ int mosp_sosp_from_scratch(mosp_workspace *ws, int n, int m, const int *d_out_ro
   if ((st = queueEngine(ws, p, 0, s)) != MOSP_OK) return st;
   if ((st = readControl(ws, 0, 1, s)) != MOSP_OK) return st;
   const EngineControl &c = ws->hostCtl[0];
+  ws->heavySeen[0] = c.heavy != 0;
   if ((st = controlStatus(ws, c)) != MOSP_OK) return st;
   if (stats) fillStats(c, 0, bits, stats);
   return maybeResetGenerations(ws, c.finalGen, s);
@@ -1066,6 +1150,7 @@ int mosp_combined_sosp(mosp_workspace *ws, int n, int K, const int *d_parents, c
   if ((st = readControl(ws, 1, 1, s)) != MOSP_OK) return st;
   readEvents(ws, nullptr, &ws->lastCombinedMs);
   const EngineControl &c = ws->hostCtl[1];
+  ws->heavySeen[1] = c.heavy != 0;
   if ((st = controlStatus(ws, c)) != MOSP_OK) return st;
   if (stats) {
     stats->edges = static_cast<int>(c.sums[0]);
@@ -1134,6 +1219,8 @@ int mosp_update_device(mosp_workspace *ws, int n, int m, int K, const int *d_out
     if ((st = readControl(ws, 0, 2, s)) != MOSP_OK) return st;
   }
   readEvents(ws, &ws->lastUpdateMs, &ws->lastCombinedMs);
+  ws->heavySeen[0] = ws->hostCtl[0].heavy != 0;
+  ws->heavySeen[1] = ws->hostCtl[1].heavy != 0;
   if ((st = controlStatus(ws, ws->hostCtl[0])) != MOSP_OK) return st;
   if ((st = controlStatus(ws, ws->hostCtl[1])) != MOSP_OK) return st;
   const EngineControl &cu = ws->hostCtl[0];

@@ -69,6 +69,28 @@ __device__ __forceinline__ int ldVolatile(const int *p) {
   return *reinterpret_cast<const volatile int *>(p);
 }
 
+__device__ __forceinline__ unsigned ldVolatileU(const unsigned *p) {
+  return *reinterpret_cast<const volatile unsigned *>(p);
+}
+
+__device__ __forceinline__ unsigned long long ldAcquire64(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void stRelease64(unsigned long long *p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ void stRelaxed64(unsigned long long *p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ void redRelease(unsigned *p, unsigned v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 /// Word helpers for one objective.
 struct Pk {
   int bits;
@@ -225,10 +247,7 @@ enum : int { kDone = 0, kPush = 1, kSplit = 2 };
 // CTA and list instead of one per warp group on the relaxation's critical
 // path. Entries that do not fit the buffer take the direct global path.
 // ---------------------------------------------------------------------------
-#ifndef MOSP_STAGE_ENTRIES
-#define MOSP_STAGE_ENTRIES 8192
-#endif
-constexpr int kStage = MOSP_STAGE_ENTRIES;
+constexpr int kStage = kStageEntriesMax;
 // Rows with more edges than this are expanded (push) or reduced (pull) by a
 // whole CTA instead of one warp: a power-law hub row (10^5 edges) would
 // otherwise keep one warp busy for the whole iteration. A launch turns
@@ -256,6 +275,7 @@ struct StageHeader {
   int heavyDeg[kHeavyCap];
   u64 heavyD[kHeavyCap];       // push: the row's distance; pull: the word before the pass
   u64 heavyBest[kHeavyCap];    // pull: best word over the row, reduced by the CTA
+  int asyncFar[kThreads / 32]; // async loop: entries in each warp's far buffer
 };
 
 struct StageEntry {
@@ -266,6 +286,11 @@ struct StageEntry {
 
 constexpr size_t kStageHeaderBytes = (sizeof(StageHeader) + 15) / 16 * 16;
 constexpr size_t kStageBytes = kStageHeaderBytes + kStage * sizeof(StageEntry);
+
+/// Dynamic shared memory of a launch with `entries` stage entries.
+constexpr size_t stageBytesFor(int entries) {
+  return kStageHeaderBytes + static_cast<size_t>(entries) * sizeof(StageEntry);
+}
 
 __device__ __forceinline__ StageHeader &stageHeader() {
   extern __shared__ __align__(16) unsigned char dynSmem[];
@@ -380,6 +405,137 @@ __device__ void flushStage(const EngineParams &P, const LoopShared &L, int wrSlo
 #endif
 constexpr int kSlots = MOSP_EDGE_SLOTS;
 
+// ---------------------------------------------------------------------------
+// Asynchronous near queue
+//
+// In the asynchronous loop the near entries of all objectives go to one
+// queue of aqShards shards. An entry is one 64-bit word: the vertex and its
+// objective (v << 5 | k) in the low half and the distance it was pushed with
+// (saturated at kTagSat) in the high half; an empty slot holds all ones, so a
+// consumer that claimed a slot before its entry was written sees it arrive.
+// A warp reserves slots for the entries of one round with one atomic on the
+// target shard's tail (shards rotate per round, which spreads the work), and
+// claims 32 slots of its home shard with one atomic on the head; it settles
+// what it consumed with one release add on the shard's `done` after its own
+// reservations, so done == tail on every shard (read twice, identical) means
+// that no entry is left and none can be produced. A reservation past the
+// shard's capacity moves its vertex to the far pile instead (re-split in the
+// next phase), so the queue never needs more than its fixed size.
+// ---------------------------------------------------------------------------
+constexpr unsigned long long kEmptySlot = ~0ULL;
+constexpr unsigned kTagSat = 0xFFFFFFFEu;  // distances >= this are not carried in the entry
+constexpr int kFarBuf = 128;               // per-warp far buffer entries (async loop)
+constexpr int kWarps = kThreads / 32;
+
+struct AsyncState {
+  AsyncShard *ctr;   // this phase's counter set
+  int target;        // shard that receives this warp round's near entries
+  unsigned spilled;  // this lane's reservations past the shard's capacity
+};
+
+/// Per-warp buffers of far-pile appends in the async loop (v << 5 | k), in
+/// the stage region of the dynamic shared memory.
+__device__ __forceinline__ int *asyncFarBuffer(int warp) {
+  return reinterpret_cast<int *>(stageEntries()) + warp * kFarBuf;
+}
+
+/// Far-pile append in the async loop: into the warp's buffer (flushed by
+/// flushAsyncFar before it can overflow), the CTA's far minimum in shared
+/// memory. An append that finds the buffer full goes to the pile directly.
+__device__ __forceinline__ void asyncFar(const EngineParams &P, const LoopShared &L, int k, int w,
+                                         u64 d) {
+  StageHeader &H = stageHeader();
+  const int warp = threadIdx.x >> 5;
+  atomicMin(&H.farMin[k], d);
+  const int slot = atomicAdd(&H.asyncFar[warp], 1);
+  if (slot < kFarBuf) {
+    asyncFarBuffer(warp)[slot] = (w << 5) | k;
+  } else {
+    const Target t = listTarget(P, L, P.K + k, 0, nullptr, nullptr);
+    const int idx = warpAppend(t.counter);
+    t.v[idx] = w;
+  }
+}
+
+/// The warp's buffered far appends to their piles (one reservation per
+/// objective group of lanes). All 32 lanes call it.
+__device__ void flushAsyncFar(const EngineParams &P, const LoopShared &L) {
+  StageHeader &H = stageHeader();
+  const int warp = threadIdx.x >> 5;
+  const unsigned lane = laneId();
+  __syncwarp();
+  int cnt = H.asyncFar[warp];
+  cnt = cnt < kFarBuf ? cnt : kFarBuf;
+  const int *buf = asyncFarBuffer(warp);
+  for (int i0 = 0; i0 < cnt; i0 += 32) {
+    const int i = i0 + static_cast<int>(lane);
+    if (i < cnt) {
+      const int e = buf[i];
+      const int k = e & 31;
+      const int v = static_cast<int>(static_cast<unsigned>(e) >> 5);
+      const Target t = listTarget(P, L, P.K + k, 0, nullptr, nullptr);
+      const int idx = warpAppend(t.counter);
+      t.v[idx] = v;
+    }
+  }
+  __syncwarp();
+  if (lane == 0) H.asyncFar[warp] = 0;
+  __syncwarp();
+}
+
+/// Whether the warp's far buffer has fewer than `margin` free entries; the
+/// same answer in every lane (all 32 lanes call it).
+__device__ __forceinline__ bool farBufferFull(int margin) {
+  __syncwarp();
+  const int cnt = __shfl_sync(kFull, stageHeader().asyncFar[threadIdx.x >> 5], 0);
+  return cnt > kFarBuf - margin;
+}
+
+/// Near-queue push of (w, d) for objective k into the round's target shard.
+/// The active lanes share one reservation.
+__device__ __forceinline__ void asyncNear(const EngineParams &P, const LoopShared &L, AsyncState &A,
+                                          int k, int w, u64 d) {
+  const unsigned mask = __activemask();
+  const unsigned lane = laneId();
+  const int leader = __ffs(mask) - 1;
+  unsigned base = 0;
+  if (static_cast<int>(lane) == leader) base = atomicAdd(&A.ctr[A.target].tail, __popc(mask));
+  base = __shfl_sync(mask, base, leader);
+  const unsigned idx = base + __popc(mask & ((1u << lane) - 1u));
+  if (idx < P.aqShardCap) {
+    const unsigned tag = d < kTagSat ? static_cast<unsigned>(d) : kTagSat;
+    const u64 e = (static_cast<u64>(tag) << 32) | ((static_cast<unsigned>(w) << 5) | static_cast<unsigned>(k));
+    u64 *slot = P.aqSlots + static_cast<long long>(A.target) * P.aqShardCap + idx;
+    // A consumer expands with min(tag, its read of the word), so only an
+    // entry without a usable tag needs the word ordered before it.
+    if (tag < kTagSat) stRelaxed64(slot, e); else stRelease64(slot, e);
+  } else {
+    ++A.spilled;
+    if (atomicExch(P.inFar + static_cast<long long>(k) * P.stride + w, 1) == 0) asyncFar(P, L, k, w, d);
+  }
+}
+
+/// A strict improvement of w's distance to d (objective k): to the next near
+/// list (d below the threshold) or, once, to the far pile.
+template <bool Async>
+__device__ __forceinline__ void pushImproved(const EngineParams &P, const LoopShared &L, AsyncState *A,
+                                             int k, int w, u64 d, int wrSlot, int *nearWV,
+                                             u64 *nearWD) {
+  if (d < L.thr[k]) {
+    if constexpr (Async) {
+      asyncNear(P, L, *A, k, w, d);
+    } else {
+      stageAppend(P, L, k, w, d, wrSlot, nearWV, nearWD);
+    }
+  } else if (atomicExch(P.inFar + static_cast<long long>(k) * P.stride + w, 1) == 0) {
+    if constexpr (Async) {
+      asyncFar(P, L, k, w, d);
+    } else {
+      stageAppend(P, L, P.K + k, w, d, wrSlot, nearWV, nearWD);
+    }
+  }
+}
+
 /// Lane of the warp whose edge range holds edge slot s: the number of
 /// lanes whose inclusive edge count is <= s (binary search by shuffles).
 __device__ __forceinline__ int slotOwner(int incl, int s) {
@@ -407,11 +563,7 @@ __device__ __forceinline__ void relaxEdge(const EngineParams &P, const LoopShare
   if (w == P.source || nd > O.maxDist) return;
   const u64 old = atomicMin(P.packed + ko + w, pk.pack(nd, u));
   if (nd >= pk.dist(old)) return;
-  if (nd < L.thr[k]) {
-    stageAppend(P, L, k, w, nd, wrSlot, nearWV, nearWD);
-  } else if (atomicExch(P.inFar + ko + w, 1) == 0) {
-    stageAppend(P, L, P.K + k, w, nd, wrSlot, nearWV, nearWD);
-  }
+  pushImproved<false>(P, L, nullptr, k, w, nd, wrSlot, nearWV, nearWD);
 }
 
 /// The CTA's queued heavy rows, each expanded by all threads of the CTA.
@@ -445,15 +597,14 @@ __device__ void expandHeavy(const EngineParams &P, const LoopShared &L, const in
 /// with their loads and 64-bit atomicMin overlapped; every strict
 /// improvement is staged for the next near list or the far pile. All 32
 /// lanes call it.
-template <int Mode>
+template <int Mode, bool Async = false>
 __device__ __forceinline__ void expandWarp(const EngineParams &P, const LoopShared &L,
                                            const int *outRow, const int *outCol,
                                            const int *const *outWk, int k, int u, u64 du, int beg,
                                            int deg, int wrSlot, int *nearWV, u64 *nearWD,
-                                           bool heavyOn) {
+                                           bool heavyOn, AsyncState *A = nullptr) {
   StageHeader &H = stageHeader();
   const unsigned lane = laneId();
-  const int K = P.K;
   {
     // statistics: one shared add per objective present in the warp
     const unsigned live = __ballot_sync(kFull, u >= 0);
@@ -498,11 +649,7 @@ __device__ __forceinline__ void expandWarp(const EngineParams &P, const LoopShar
       if (w == P.source || nd > O.maxDist) continue;
       const u64 old = atomicMin(P.packed + kob + w, pk.pack(nd, ub));
       if (nd >= pk.dist(old)) continue;
-      if (nd < L.thr[kb]) {
-        stageAppend(P, L, kb, w, nd, wrSlot, nearWV, nearWD);
-      } else if (atomicExch(P.inFar + kob + w, 1) == 0) {
-        stageAppend(P, L, K + kb, w, nd, wrSlot, nearWV, nearWD);
-      }
+      pushImproved<Async>(P, L, A, kb, w, nd, wrSlot, nearWV, nearWD);
     }
   }
   if (deg > (1 << 20)) deg = 0;
@@ -515,6 +662,10 @@ __device__ __forceinline__ void expandWarp(const EngineParams &P, const LoopShar
   const int edges = __shfl_sync(kFull, incl, 31);
   const int excl = incl - deg;
   for (int s0 = 0; s0 < edges; s0 += 32 * kSlots) {
+    if constexpr (Async) {
+      // room for this round's far appends in the warp's buffer
+      if (farBufferFull(32 * kSlots)) flushAsyncFar(P, L);
+    }
     // kSlots edge slots per lane, their loads and atomics overlapped
     int sl[kSlots], kk[kSlots], uu[kSlots], ee[kSlots], ww[kSlots], wt[kSlots];
     u64 dd[kSlots], nd[kSlots], old[kSlots];
@@ -558,11 +709,7 @@ __device__ __forceinline__ void expandWarp(const EngineParams &P, const LoopShar
 #pragma unroll
     for (int h = 0; h < kSlots; ++h) {
       if (!act[h] || nd[h] >= pkOf(P.obj[kk[h]]).dist(old[h])) continue;
-      if (nd[h] < L.thr[kk[h]]) {
-        stageAppend(P, L, kk[h], ww[h], nd[h], wrSlot, nearWV, nearWD);
-      } else if (atomicExch(P.inFar + static_cast<long long>(kk[h]) * P.stride + ww[h], 1) == 0) {
-        stageAppend(P, L, K + kk[h], ww[h], nd[h], wrSlot, nearWV, nearWD);
-      }
+      pushImproved<Async>(P, L, A, kk[h], ww[h], nd[h], wrSlot, nearWV, nearWD);
     }
   }
 }
@@ -617,7 +764,7 @@ __device__ bool nearFarLoop(const EngineParams &P, const int *outRow,
     }
     if (threadIdx.x < kMaxK) H.farMin[threadIdx.x] = kInfWord;
     if (threadIdx.x == 0) {
-      H.cap = kStage / (2 * K);
+      H.cap = P.stageEntries / (2 * K);
       H.heavyCount = 0;
     }
     if (warp == 0) {
@@ -834,6 +981,303 @@ __device__ bool nearFarLoop(const EngineParams &P, const int *outRow,
         c->loopItems[q] = profItems[q];
       }
       for (int q = 0; q < 5; ++q) c->iterSplitNs[q] = part[q];
+    }
+  }
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// Asynchronous near-far loop
+//
+// The bulk loop above pays a grid barrier per iteration and, worse, waits in
+// every iteration for the slowest warp of the grid. Here a phase runs one
+// far-pile split and then expands the near entries asynchronously: every
+// warp claims slots of the near queue, expands what has arrived and pushes
+// what improves, with no barrier until the whole phase has run dry. Only the
+// split of the far piles (a new threshold per objective) needs the grid to
+// agree, so there is one grid barrier per phase (a few per launch) instead
+// of one per iteration (80-150). Relaxations are the same monotone 64-bit
+// atomicMin, so the fixed point, i.e. every word, is the one the bulk loop
+// reaches.
+// ---------------------------------------------------------------------------
+
+/// Phase end detection (warp 0 of CTA 0 while it is idle): every CTA has
+/// finished its split and, in two successive reads of all shards' counters,
+/// done == tail everywhere with nothing changed in between (the counters
+/// only grow, so the second read shows the state of one moment).
+__device__ void detectPhaseEnd(const EngineParams &P, const AsyncShard *ctr, unsigned phase) {
+  EngineControl *c = P.ctl;
+  const unsigned lane = laneId();
+  const int S = P.aqShards;
+  unsigned split = 0;
+  if (lane == 0) split = ldAcquire(&c->asyncSplit);
+  split = __shfl_sync(kFull, split, 0);
+  if (split < (phase + 1) * gridDim.x) return;
+  unsigned d1 = 0, t1 = 0, d2 = 0, t2 = 0;
+  if (static_cast<int>(lane) < S) {
+    d1 = ldAcquire(&ctr[lane].done);
+    t1 = ldAcquire(&ctr[lane].tail);
+  }
+  if (!__all_sync(kFull, d1 == t1)) return;
+  if (static_cast<int>(lane) < S) {
+    d2 = ldAcquire(&ctr[lane].done);
+    t2 = ldAcquire(&ctr[lane].tail);
+  }
+  if (!__all_sync(kFull, d2 == d1 && t2 == t1)) return;
+  if (lane == 0) stRelease(&c->asyncPhase, phase + 1);
+}
+
+/// Settle one warp round: `consumed` entries of shard `from` and the lanes'
+/// reservations past the capacity of shard `to`, after the round's own
+/// reservations (release).
+__device__ __forceinline__ void settleRound(AsyncShard *ctr, int from, unsigned consumed, int to,
+                                            unsigned spilled) {
+  if (__any_sync(kFull, spilled != 0)) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) spilled += __shfl_xor_sync(kFull, spilled, off);
+  }
+  if (consumed == 0 && spilled == 0) return;  // the same in every lane
+  __syncwarp();
+  if (laneId() == 0) {
+    __threadfence();
+    if (consumed != 0) redRelease(&ctr[from].done, consumed);
+    if (spilled != 0) redRelease(&ctr[to].done, spilled);
+  }
+}
+
+/// The consumer side of one phase for one warp: claim slots, expand the
+/// entries that arrive, until the phase is over (true) or the launch is
+/// stopped (false).
+template <int Mode>
+__device__ bool asyncConsume(const EngineParams &P, const LoopShared &L, const int *outRow,
+                             const int *outCol, const int *const *outWk, AsyncShard *ctr,
+                             unsigned phase, long long gwarp, const Sync &sync) {
+  EngineControl *c = P.ctl;
+  const unsigned lane = laneId();
+  const int S = P.aqShards;
+  const unsigned cap = P.aqShardCap;
+  int cs = static_cast<int>(gwarp % S);  // shard this warp claims from
+  int hops = 0;                          // shards found exhausted
+  int target = static_cast<int>((gwarp * 7 + 3) % S);
+  unsigned pend = 0, cb = 0, spins = 0;
+  while (true) {
+    if (pend == 0 && hops < S) {
+      unsigned b = 0;
+      if (lane == 0) b = atomicAdd(&ctr[cs].head, 32u);
+      b = __shfl_sync(kFull, b, 0);
+      if (b >= cap) {
+        cs = (cs + 1) % S;
+        ++hops;
+        continue;
+      }
+      cb = b;
+      const unsigned room = cap - b;
+      pend = room >= 32u ? kFull : ((1u << room) - 1u);
+    }
+    u64 *slot = P.aqSlots + static_cast<long long>(cs) * cap + cb + lane;
+    u64 e = kEmptySlot;
+    // only slots below the shard's tail are reserved (one load per warp
+    // instead of 32 while the warp waits for work)
+    unsigned tail = 0;
+    if (pend != 0 && lane == 0) tail = ldVolatileU(&ctr[cs].tail);
+    tail = __shfl_sync(kFull, tail, 0);
+    if (((pend >> lane) & 1u) && cb + lane < tail) e = ldAcquire64(slot);
+    const unsigned ready = __ballot_sync(kFull, e != kEmptySlot);
+    if (ready == 0) {
+      unsigned ph = 0;
+      if (lane == 0) ph = ldAcquire(&c->asyncPhase);
+      ph = __shfl_sync(kFull, ph, 0);
+      if (ph > phase) return true;
+      if (gwarp == 0) detectPhaseEnd(P, ctr, phase);
+      if ((++spins & 63u) == 0) {
+        int stop = 0;
+        if (lane == 0) {
+          stop = ldVolatile(&c->status) != 0;
+          if (!stop && globalNs() > sync.deadline) {
+            atomicCAS(&c->status, 0, MOSP_ERR_TIMEOUT);
+            stop = 1;
+          }
+        }
+        if (__shfl_sync(kFull, stop, 0)) return false;
+      }
+      __nanosleep(spins < 32 ? 32 : 256);
+      continue;
+    }
+    spins = 0;
+    pend &= ~ready;
+    int k = 0, u = -1, beg = 0, deg = 0;
+    u64 du = 0;
+    if (e != kEmptySlot) {
+      stRelaxed64(slot, kEmptySlot);
+      const unsigned vk = static_cast<unsigned>(e);
+      const unsigned tag = static_cast<unsigned>(e >> 32);
+      k = static_cast<int>(vk & 31u);
+      const int v = static_cast<int>(vk >> 5);
+      const u64 word = __ldcg(P.packed + static_cast<long long>(k) * P.stride + v);
+      const int b0 = ldGraph<Mode>(outRow + v);
+      const int b1 = ldGraph<Mode>(outRow + v + 1);
+      const u64 d = word == kInfWord ? kInfWord : pkOf(P.obj[k]).dist(word);
+      // stale (a later, smaller distance has its own entry) unless d >= tag;
+      // a word read older than the entry is covered by expanding with the tag
+      if (tag < kTagSat) {
+        if (d >= tag) {
+          u = v;
+          du = tag;
+        }
+      } else if (d != kInfWord) {
+        u = v;
+        du = d;
+      }
+      if (u >= 0) {
+        beg = b0;
+        deg = b1 - b0;
+      }
+    }
+    AsyncState A{ctr, target, 0u};
+    expandWarp<Mode, true>(P, L, outRow, outCol, outWk, k, u, du, beg, deg, 0, nullptr, nullptr,
+                           false, &A);
+    settleRound(ctr, cs, __popc(ready), target, A.spilled);
+    target = target + 1 == S ? 0 : target + 1;
+  }
+}
+
+template <int Mode>
+__device__ bool asyncNearFar(const EngineParams &P, const int *outRow, const int *outCol,
+                             const int *const *outWk, Sync &epoch, u64 *deltaOverride, int genBase) {
+  __shared__ LoopShared L;
+  StageHeader &H = stageHeader();
+  EngineControl *c = P.ctl;
+  const int K = P.K;
+  const int S = P.aqShards;
+  const unsigned lane = laneId();
+  const int warp = threadIdx.x >> 5;
+  const long long gwarp = static_cast<long long>(blockIdx.x) * (blockDim.x >> 5) + warp;
+  const long long nwarps = static_cast<long long>(gridDim.x) * (blockDim.x >> 5);
+
+  // per-objective state, held by lane k of warp 0 (the same in every CTA)
+  u64 thr = 0;
+  int fp = 0, fs = 0, phasesK = 0;
+  u64 delta = 1;
+  if (warp == 0 && static_cast<int>(lane) < K) {
+    delta = P.obj[lane].delta;
+    if (deltaOverride != nullptr && lane == 0) delta = *deltaOverride;
+  }
+  if (threadIdx.x < kMaxK) H.expanded[threadIdx.x] = 0;
+  if (threadIdx.x < kWarps) H.asyncFar[threadIdx.x] = 0;
+  const unsigned long long t0 = globalNs();
+  unsigned phase = 0;
+  for (;; ++phase) {
+    if (threadIdx.x < kMaxK) H.farMin[threadIdx.x] = kInfWord;
+    if (warp == 0) {
+      const int k = static_cast<int>(lane);
+      const bool act = k < K;
+      int mode = kDone;
+      long long items = 0;
+      if (act) {
+        const int fc = __ldcg(&c->farCount[k][fs]);
+        if (fc > 0) {
+          mode = kSplit;
+          items = fc;
+          const u64 mnC = __ldcg(&c->farMinC[k][fs]);
+          u64 lo = thr;
+          if (mnC != 0) {
+            const u64 mn = ~mnC;
+            lo = mn > thr ? mn : thr;
+          }
+          thr = (lo > kInfWord - delta) ? kInfWord - 1 : lo + delta;
+        }
+      }
+      long long incl = items;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const long long o = __shfl_up_sync(kFull, incl, off);
+        if (static_cast<int>(lane) >= off) incl += o;
+      }
+      if (act) {
+        L.off[k] = incl - items;
+        L.thr[k] = thr;
+        L.mode[k] = mode;
+        L.fp[k] = fp;
+        L.fs[k] = fs;
+      }
+      const long long total = __shfl_sync(kFull, incl, 31);
+      if (lane == 0) L.total = total;
+      if (act && mode == kSplit) {
+        if (blockIdx.x == 0) {
+          c->farCount[k][(fs + 2) % 3] = 0;
+          c->farMinC[k][(fs + 2) % 3] = 0;
+        }
+        ++phasesK;
+        fp ^= 1;
+        fs = (fs + 1) % 3;
+      }
+    }
+    // the counter set of the next phase (last used two phases ago)
+    if (blockIdx.x == 0 && static_cast<int>(threadIdx.x) < S) {
+      AsyncShard &nx = P.aqCtr[((phase + 1) & 1u) * S + threadIdx.x];
+      nx.head = 0;
+      nx.tail = 0;
+      nx.done = 0;
+    }
+    __syncthreads();
+    const long long total = L.total;
+    if (total == 0) break;
+    AsyncShard *ctr = P.aqCtr + (phase & 1u) * S;
+
+    // ---- split: this warp's share of the far piles, below the new
+    // threshold to the near queue, the rest to the other pile
+    {
+      AsyncState A{ctr, static_cast<int>(gwarp % S), 0u};
+      for (long long base = gwarp * 32; base < total; base += nwarps * 32) {
+        if (farBufferFull(32)) flushAsyncFar(P, L);
+        const long long j = base + lane;
+        if (j < total) {
+          int k = 0;
+          while (k + 1 < K && L.off[k + 1] <= j) ++k;
+          const long long ko = static_cast<long long>(k) * P.stride;
+          const int v = __ldcg((L.fp[k] == 0 ? P.farL0 : P.farL1) + ko + (j - L.off[k]));
+          const u64 word = __ldcg(P.packed + ko + v);
+          const u64 d = word == kInfWord ? kInfWord : pkOf(P.obj[k]).dist(word);
+          if (d < L.thr[k]) {
+            P.inFar[ko + v] = 0;
+            asyncNear(P, L, A, k, v, d);
+          } else {
+            asyncFar(P, L, k, v, d);
+          }
+        }
+        settleRound(ctr, 0, 0u, A.target, A.spilled);
+        A.spilled = 0;
+        A.target = A.target + 1 == S ? 0 : A.target + 1;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      redRelease(&c->asyncSplit, 1u);
+    }
+
+    // ---- expand until the phase runs dry
+    if (!asyncConsume<Mode>(P, L, outRow, outCol, outWk, ctr, phase, gwarp, epoch)) return false;
+    flushAsyncFar(P, L);
+    __syncthreads();
+    if (threadIdx.x < K && H.farMin[threadIdx.x] != kInfWord) {
+      atomicMax(listTarget(P, L, K + threadIdx.x, 0, nullptr, nullptr).minC, ~H.farMin[threadIdx.x]);
+    }
+    if (!gridSync(c, epoch)) return false;
+  }
+
+  if (threadIdx.x < K && H.expanded[threadIdx.x] != 0) {
+    atomicAdd(reinterpret_cast<unsigned long long *>(&c->pushes[threadIdx.x]),
+              static_cast<unsigned long long>(H.expanded[threadIdx.x]));
+  }
+  if (blockIdx.x == 0 && warp == 0 && static_cast<int>(lane) < K) {
+    c->iterations[lane] = phasesK;
+    c->epochs[lane] = phasesK;
+    if (lane == 0) {
+      c->finalGen = genBase + 1;
+      *P.genPtr = genBase + 1;
+      c->loopNs[0] = globalNs() - t0;
+      c->loopIters[0] = phase;
     }
   }
   return true;
@@ -1071,6 +1515,20 @@ template <int Mode>
 __device__ void scratchOrCombined(const EngineParams &P, Sync &epoch, int genBase,
                                   const int **sOutWk);
 
+/// The near-far loop of a launch: asynchronous when the launch asks for it
+/// and the graph has no hub rows (which the bulk loop hands to whole CTAs);
+/// the same decision in every CTA (the hub flag is set before a barrier).
+template <int Mode>
+__device__ bool runNearFar(const EngineParams &P, const int *outRow, const int *outCol,
+                           const int *const *outWk, Sync &epoch, u64 *deltaOverride, int genBase) {
+  const bool async = (P.flags & kFlagAsync) != 0 && P.aqSlots != nullptr && P.aqShards > 0 &&
+                     P.aqShards <= kAsyncShards && P.n <= (1 << 27) &&
+                     P.stageEntries * sizeof(StageEntry) >= kWarps * kFarBuf * sizeof(int) &&
+                     __ldcg(&P.ctl->heavy) == 0;
+  if (async) return asyncNearFar<Mode>(P, outRow, outCol, outWk, epoch, deltaOverride, genBase);
+  return nearFarLoop<Mode>(P, outRow, outCol, outWk, epoch, deltaOverride, genBase);
+}
+
 // ---------------------------------------------------------------------------
 // The engine kernel
 // ---------------------------------------------------------------------------
@@ -1127,6 +1585,15 @@ __global__ void __launch_bounds__(kThreads, 1) sospEngine(const __grid_constant_
   const int *outCol = P.outCol;
 
   markPhase(c, kPhaseStart);
+  // both counter sets of the asynchronous near queue start at zero (every
+  // mode passes a grid barrier before its near-far loop)
+  if ((P.flags & kFlagAsync) != 0 && P.aqCtr != nullptr) {
+    for (long long i = tid; i < 2LL * P.aqShards; i += T) {
+      P.aqCtr[i].head = 0;
+      P.aqCtr[i].tail = 0;
+      P.aqCtr[i].done = 0;
+    }
+  }
   if constexpr (Mode == kModeUpdate) {
     // ---- Heavy rows: does the graph have rows for whole-CTA handling? -----
     for (long long v = tid; v < n; v += T) {
@@ -1297,7 +1764,7 @@ __global__ void __launch_bounds__(kThreads, 1) sospEngine(const __grid_constant_
         H.farMin[threadIdx.x] = kInfWord;
       }
       if (threadIdx.x == 0) {
-        H.cap = kStage / K;
+        H.cap = P.stageEntries / K;
         H.heavyCount = 0;
       }
       __syncthreads();
@@ -1305,11 +1772,11 @@ __global__ void __launch_bounds__(kThreads, 1) sospEngine(const __grid_constant_
       // set in the first phase, the same for every thread of the grid
       const bool heavyOn = __ldcg(&c->heavy) != 0;
       // Improved candidates go to far pile 0. With a partition of at least
-      // one tile per objective (K * blockDim <= kStage) the appends are
+      // one tile per objective (K * blockDim <= stage entries) the appends are
       // staged per CTA and written out with one reservation per objective
       // when a partition could fill up and at the end; otherwise each warp
       // appends to the global pile directly.
-      const bool staged = K * static_cast<int>(blockDim.x) <= kStage;
+      const bool staged = K * static_cast<int>(blockDim.x) <= P.stageEntries;
       auto flushPull = [&]() {
         __syncthreads();
         if (threadIdx.x < K && H.count[threadIdx.x] > 0) {
@@ -1464,7 +1931,7 @@ __global__ void __launch_bounds__(kThreads, 1) sospEngine(const __grid_constant_
     }
     if (!gridSync(c, epoch)) return;
     markPhase(c, kPhasePulled);
-    if (!nearFarLoop<Mode>(P, outRow, outCol, sOutWk, epoch, nullptr, genBase)) return;
+    if (!runNearFar<Mode>(P, outRow, outCol, sOutWk, epoch, nullptr, genBase)) return;
     markPhase(c, kPhaseLoop);
     unpackResults<Mode>(P, outRow, outCol, sOutWk, epoch);
     if (!gridSync(c, epoch)) return;
@@ -1561,6 +2028,22 @@ __device__ void scratchOrCombined(const EngineParams &P, Sync &epoch, int genBas
     // fall through to the SSSP from scratch
   }
 
+  if constexpr (Mode == kModeScratch) {
+    // The caller's CSR is checked before any access that it indexes: row
+    // offsets monotone from 0 to m, every column in [0, n). A malformed graph
+    // ends the launch with `invalid` set, before the relaxations.
+    if (tid == 0 && (__ldg(outRow) != 0 || __ldg(outRow + n) != P.m)) c->invalid = 1;
+    for (long long v = tid; v < n; v += T) {
+      if (__ldg(outRow + v + 1) < __ldg(outRow + v)) c->invalid = 1;
+    }
+    for (long long e = tid; e < P.m; e += T) {
+      const int x = __ldg(outCol + e);
+      if (x < 0 || x >= n) c->invalid = 1;
+    }
+    if (!gridSync(c, epoch)) return;
+    if (__ldcg(&c->invalid) != 0) return;
+  }
+
   // ---- SSSP from scratch: only the source (the roots) is finite ------------
   for (long long v = tid; v < n; v += T) {
     if (ldGraph<Mode>(outRow + v + 1) - ldGraph<Mode>(outRow + v) > kHeavyDeg) c->heavy = 1;
@@ -1587,7 +2070,7 @@ __device__ void scratchOrCombined(const EngineParams &P, Sync &epoch, int genBas
   markPhase(c, kPhasePulled);
   u64 *deltaOverride = nullptr;
   if constexpr (Mode == kModeCombined) deltaOverride = &sCombDelta;
-  if (!nearFarLoop<Mode>(P, outRow, outCol, sOutWk, epoch, deltaOverride, genBase)) return;
+  if (!runNearFar<Mode>(P, outRow, outCol, sOutWk, epoch, deltaOverride, genBase)) return;
   markPhase(c, kPhaseLoop);
   unpackResults<Mode>(P, outRow, outCol, sOutWk, epoch);
   if (!gridSync(c, epoch)) return;
@@ -1868,7 +2351,8 @@ cudaError_t launchEngine(const EngineParams &p, int ctas, cudaStream_t s) {
     case kModeScratch: fn = reinterpret_cast<const void *>(sospEngine<kModeScratch>); break;
     default: fn = reinterpret_cast<const void *>(sospEngine<kModeCombined>); break;
   }
-  return cudaLaunchCooperativeKernel(fn, dim3(ctas), dim3(kThreads), args, kStageBytes, s);
+  return cudaLaunchCooperativeKernel(fn, dim3(ctas), dim3(kThreads), args,
+                                     stageBytesFor(p.stageEntries), s);
 }
 
 bool needsHostRecovery(const EngineParams &p) {
@@ -1892,7 +2376,7 @@ cudaError_t launchEngineEx(const EngineParams &p, int ctas, cudaStream_t s) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(ctas);
   cfg.blockDim = dim3(kThreads);
-  cfg.dynamicSmemBytes = kStageBytes;
+  cfg.dynamicSmemBytes = stageBytesFor(p.stageEntries);
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeCooperative;

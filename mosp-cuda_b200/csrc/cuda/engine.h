@@ -25,6 +25,13 @@ constexpr int kMaxK = MOSP_MAX_OBJECTIVES;    // objectives per launch
 constexpr u64 kInfWord = ~0ULL;               // packed INF (all ones)
 constexpr long long kDistInf = MOSP_DISTANCE_INF;
 constexpr int kLaneRowMax = 32;               // rows above: warp-cooperative
+#ifndef MOSP_STAGE_ENTRIES
+#define MOSP_STAGE_ENTRIES 8192
+#endif
+// entries of the per-CTA append stage of a bulk near-far launch (16 bytes
+// each, dynamic shared memory); asynchronous launches take fewer
+constexpr int kStageEntriesMax = MOSP_STAGE_ENTRIES;
+constexpr int kStageEntriesAsync = 1024;     // the far buffers of 32 warps
 
 enum EngineMode : int { kModeUpdate = 0, kModeScratch = 1, kModeCombined = 2 };
 
@@ -52,6 +59,10 @@ struct alignas(128) EngineControl {
   unsigned pad0[31];
   unsigned release;      // barrier epoch released by the last arrival
   unsigned pad1[31];
+  unsigned asyncPhase;   // asynchronous near-far: phases completed (monotone)
+  unsigned pad3[31];
+  unsigned asyncSplit;   // asynchronous near-far: CTAs past their phase's split (monotone)
+  unsigned pad4[31];
   int status;            // 0 or MOSP_ERR_TIMEOUT (run aborted)
   int overflow;          // an input distance does not fit the packing
   int invalid;           // malformed input (ids out of range, cycles)
@@ -85,9 +96,28 @@ struct alignas(128) EngineControl {
 // EngineParams::flags (tuning switches; results do not depend on them)
 enum : int {
   kFlagPrecheck = 1,     // read the word before the atomicMin of a relaxation
-  kFlagHostRecovery = 2  // leave the lowest-id parent recovery of distance-only
+  kFlagHostRecovery = 2, // leave the lowest-id parent recovery of distance-only
                          // objectives to recoverParents, launched right after
+  kFlagAsync = 4         // asynchronous near-far loop (one grid barrier per far-pile
+                         // split instead of one per iteration) when the graph has
+                         // no hub rows
 };
+
+/// Counters of one shard of the asynchronous near queue, each on its own
+/// 128-byte line: `head` is advanced by the warps that claim slots, `tail`
+/// by the warps that reserve slots for new entries, `done` counts the
+/// reserved entries that are settled (expanded, skipped as stale, or moved to
+/// the far pile because the shard was full). A phase is over when every
+/// shard has done == tail.
+struct alignas(128) AsyncShard {
+  unsigned head;
+  unsigned pad0[31];
+  unsigned tail;
+  unsigned pad1[31];
+  unsigned done;
+  unsigned pad2[31];
+};
+constexpr int kAsyncShards = 32;  // shards of the near queue (one counter set)
 
 // Phase boundaries recorded in EngineControl::phaseNs.
 enum : int {
@@ -125,6 +155,14 @@ struct EngineParams {
   int *nearV0, *nearV1;        // near lists: vertices
   u64 *nearD0, *nearD1;        // near lists: distance when appended
   long long stride, strideNear;
+  // asynchronous near queue (kFlagAsync): aqShards shards of aqShardCap
+  // slots, every slot ~0 (empty) between launches; two counter sets of
+  // aqShards shards (phase parity)
+  u64 *aqSlots;
+  AsyncShard *aqCtr;
+  unsigned aqShardCap;
+  int aqShards;
+  int stageEntries;            // entries of the per-CTA append stage (dynamic shared memory)
   EngineControl *ctl;
   // combined graph (Steps 2-3)
   const int *combParents;      // K trees, objective-major

@@ -59,9 +59,13 @@ constexpr long long kScratchBytes = kOffInts + kIntLists * roundUp(kMaxVertices 
 // counter, stamps, in-far flags) are cleared again by every call.
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
+// Launch shape per device ordinal (an occupancy query, made once). The
+// array's device address is looked up on every call instead: it is only
+// valid while the module stays loaded in the device's current context, and
+// a context that was torn down and created again (cudaDeviceReset) loads
+// the module anew at another address.
 struct DeviceSlot {
   bool ready = false;
-  unsigned char *base = nullptr;
   LaunchShape shape{};
 };
 DeviceSlot g_slots[kMaxDevices];
@@ -72,22 +76,24 @@ int failCuda(cudaError_t err, const char *what) {
                                        " (" + what + ")").c_str());
 }
 
-/// Address and launch shape of the current device's copy of the array.
-/// The first call on a device looks them up (module load, symbol address,
-/// occupancy query); later calls read the table.
-int setup(int &device, DeviceSlot *&slot) {
+/// Device address of the current device's copy of the array (a host-side
+/// name of a __device__ variable is not an address a kernel may use) and
+/// the launch shape. The first call on a device makes the occupancy query;
+/// every call looks the address up, with the device current.
+int setup(int &device, DeviceSlot *&slot, unsigned char *&base) {
   cudaError_t err = cudaGetDevice(&device);
   if (err != cudaSuccess) return failCuda(err, "cudaGetDevice");
   if (device < 0 || device >= kMaxDevices) {
     return recordFailure(MOSP_ERR_UNSUPPORTED,
                          "Error: mosp_sosp_from_scratch_static supports device ordinals below 64.");
   }
+  void *ptr = nullptr;
+  err = cudaGetSymbolAddress(&ptr, g_scratch);
+  if (err != cudaSuccess) return failCuda(err, "cudaGetSymbolAddress of the static scratch");
+  base = static_cast<unsigned char *>(ptr);
   std::lock_guard<std::mutex> lock(g_setupMutex);
   DeviceSlot &s = g_slots[device];
   if (!s.ready) {
-    void *ptr = nullptr;
-    err = cudaGetSymbolAddress(&ptr, g_scratch);
-    if (err != cudaSuccess) return failCuda(err, "cudaGetSymbolAddress of the static scratch");
     LaunchShape shape{};
     err = queryLaunchShape(0, shape);
     if (err == cudaErrorNotSupported) {
@@ -98,7 +104,6 @@ int setup(int &device, DeviceSlot *&slot) {
       return recordFailure(MOSP_ERR_UNSUPPORTED,
                            "Error: the launch shape exceeds the static scratch's CTA limit.");
     }
-    s.base = static_cast<unsigned char *>(ptr);
     s.shape = shape;
     s.ready = true;
   }
@@ -134,9 +139,9 @@ extern "C" int mosp_sosp_from_scratch_static(int n, int m, const int *d_out_row,
 
   int device = -1;
   DeviceSlot *slot = nullptr;
-  st = setup(device, slot);
+  unsigned char *b = nullptr;
+  st = setup(device, slot, b);
   if (st != MOSP_OK) return st;
-  unsigned char *b = slot->base;
   EngineControl *ctl = reinterpret_cast<EngineControl *>(b + kOffCtl);
   int *gen = reinterpret_cast<int *>(b + kOffGen);
   int *ints = reinterpret_cast<int *>(b + kOffInts);
@@ -166,6 +171,7 @@ extern "C" int mosp_sosp_from_scratch_static(int n, int m, const int *d_out_row,
   p.nearD0 = reinterpret_cast<u64 *>(b + kOffNearD0);
   p.nearD1 = reinterpret_cast<u64 *>(b + kOffNearD1);
   p.strideNear = kNearCap;
+  p.stageEntries = kStageEntriesMax;
   p.ctl = ctl;
   p.blockSums = reinterpret_cast<long long *>(b + kOffBlockSums);
   ObjectiveArgs &o = p.obj[0];
@@ -198,7 +204,8 @@ extern "C" int mosp_sosp_from_scratch_static(int n, int m, const int *d_out_row,
   }
   if (c.invalid) {
     return recordFailure(MOSP_ERR_INVALID,
-                         "Error: malformed input (a vertex id out of range).");
+                         "Error: malformed CSR (row offsets not monotone from 0 to m, or a column "
+                         "index outside [0, n)).");
   }
   if (stats != nullptr) {
     stats->invalidated = c.invalidated[0];

@@ -83,6 +83,7 @@ _SIGS = {
     "mosp_workspace_use_graphs": (_i, [_p, _i]),
     "mosp_workspace_set_local_rounds": (_i, [_p, _i, _i]),
     "mosp_workspace_set_narrow": (_i, [_p, _i, _i]),
+    "mosp_workspace_set_async": (_i, [_p, _i, _ll]),
     "mosp_workspace_graph_launches": (_i, [_p, _ip]),
     "mosp_autotune_update": (_i, [_p, _i, _i, _i, _p, _p, _p, _p, _p, _p, _p, _p, _ip, _p, _i, _i,
                                   _llp, _llp, _ip, _p, _p, _p, _p, _llp, _llp, _ip, C.POINTER(C.c_float), _p]),
@@ -504,6 +505,11 @@ class Workspace:
 
     def set_narrow(self, max_items, rounds):
         check(lib().mosp_workspace_set_narrow(self._h, int(max_items), int(rounds)))
+
+    def set_async(self, on=True, queue_slots=0):
+        """Asynchronous near-far loop (default) or the bulk-synchronous one;
+        queue_slots bounds the asynchronous near queue (0: default size)."""
+        check(lib().mosp_workspace_set_async(self._h, 1 if on else 0, int(queue_slots)))
 
     def use_graphs(self, on=True):
         check(lib().mosp_workspace_use_graphs(self._h, int(bool(on))))
