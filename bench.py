@@ -381,15 +381,12 @@ def run_ours(args):
         line = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-                "config": {"workload": workload, "n": n, "m": upd.m, "K": K, "changes_applied": changed,
-                           "inserts": batch.n_ins, "deletes": batch.n_del, "parallelism": f"replicas x{world}",
-                           "delta": tuned, "combined_delta": comb_delta or "default",
+                "config": shared_config(workload, n, upd.m, K, changed, batch.n_ins, batch.n_del),
+                "tuning": {"replicas": world, "delta": tuned, "combined_delta": comb_delta or "default",
                            "local_rounds": {"update": rounds[0], "combined": rounds[1]},
                            "delta_default": deltas,
                            "widths": "autotuned (mosp_autotune_update)" if args.delta <= 0 else "fixed by --delta",
-                           "l2": "flushed (256 MiB write) before every timed step",
-                           "near_far_loop": args.loop,
-                           "grid_ctas": ws.grid()},
+                           "near_far_loop": args.loop, "grid_ctas": ws.grid()},
                 "gpu_compute_ms": round(ms_per_step, 4),
                 "default_widths_ms_per_step": round(float(np.mean(default_ms)), 4),
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
@@ -760,83 +757,139 @@ def run_serving(args):
 # ---------------------------------------------------------------------------
 # reference arm: the reference's own CPU implementation of the path
 # ---------------------------------------------------------------------------
+def shared_config(workload, n, m, K, changed, n_ins, n_del):
+    """The `config` of both arms (the same dict for the same workload)."""
+    return {"workload": workload, "n": int(n), "m": int(m), "K": int(K), "changes_applied": int(changed),
+            "inserts": int(n_ins), "deletes": int(n_del),
+            "parallelism": "one process per GPU (replicas); the reference arm: one host thread per call",
+            "l2": "library arm: L2 flushed (256 MiB write) before every timed step; reference arm: host only"}
+
+
+def reference_workload(args):
+    """The library arm's workload built from oracle/ alone: the seeded graph
+    from oracle/_gen/libworkload.so (the same generator, compiled without the
+    library) and the change batch from the reference's own generateChangeBatch
+    (oracle/_ref/libref_cpu.so), which the library's generator equals byte for
+    byte. Returns (row, col, w, batch dict, K, pref, description)."""
+    import oracle as orc
+    if getattr(args, "workload", "road") == "powerlaw":
+        scale = getattr(args, "rmat_scale", 22)
+        wmax = getattr(args, "rmat_wmax", 1_000_000)
+        row, col, w = orc.workload_rmat(scale, 16, 0.57, 0.19, 0.19, 5, 1, wmax, True, 12345)
+        batch = orc.ref_generate_changes(row, col, w, 100000, 30.0, 1, 0, False, 777, 0, 1, wmax)
+        desc = POWERLAW
+        if scale != 22 or wmax != 1_000_000:
+            desc = desc.replace("R-MAT scale 22", f"R-MAT scale {scale}").replace("[1,1e6]", f"[1,{wmax}]")
+        return row, col, w, batch, 5, [1, 2, 3, 4, 5], desc
+    row, col, w = orc.workload_grid_road(args.width, args.width, 0.70, 0.01, 3, 1, 100, 12345)
+    batch = orc.ref_generate_changes(row, col, w, args.changes, 50.0, 0, 0, True, 777, 0, 1, 100)
+    return row, col, w, batch, 3, None, WORKLOAD
+
+
 def run_reference(args):
+    """The reference's CPU path on the library arm's workload, on the host
+    cores: per objective the reference's sequentialSOSPUpdate through its own
+    file API (text graph, batch and tree in, tree out), the K objectives one
+    after another as the reference runs them, then the reference's
+    combinedGraphReference + dijkstraCsrGraph on the K trees it wrote. Only
+    oracle/ libraries are loaded (the reference compiled from its sources,
+    and the workload generator); none of the library's code runs.
+
+    A step is a bounded sample: one objective's update (objective = step mod
+    K), so that W + K steps end within minutes; the combined step is timed
+    once after them. value = changed edges / (K x mean objective time +
+    combined time). The compute-only figures come from the same source
+    compiled with two clock reads around its Phases 1-2."""
     world, rank, _ = dist_setup(args)
     if rank != 0:
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
-    import mosp_b200 as mb
-    from concurrent.futures import ThreadPoolExecutor
-
-    g, batch, K, pref, workload = make_workload(args)
-    src = 0
-    row, col, w = g.arrays()
-    ba = batch.arrays()
-    changed = int(batch.n_ins + batch.n_del)
-    have_ref = orc.have_ref()
+    if not orc.have_ref():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (the reference sources "
+                                                              "were absent at build time)"}), flush=True)
+        return
+    row, col, w, batch, K, pref, workload = reference_workload(args)
+    n, src = len(row) - 1, 0
+    n_ins, n_del = len(batch["ins_from"]), len(batch["del_from"])
+    changed = n_ins + n_del
+    urow, ucol, _, _ = orc.ref_apply_batch(row, col, w, batch["ins_from"], batch["ins_to"], batch["ins_w"],
+                                           batch["del_from"], batch["del_to"])
+    m_upd = len(ucol)
     tmp = tempfile.mkdtemp(prefix="mosp_ref_")
     try:
         prefix = os.path.join(tmp, "graph", "graphCsr")
-        g.write(prefix)
+        os.makedirs(os.path.dirname(prefix))
+        orc.ref_write_csr(prefix, row, col, w)
         ins, dele = os.path.join(tmp, "insert.txt"), os.path.join(tmp, "delete.txt")
-        batch.write(ins, dele)
-        dijk = orc.ref_dijkstra if have_ref else orc.dijkstra
+        orc.ref_write_changes(ins, dele, K, batch)
         for k in range(K):
-            d, p = dijk(row, col, w, k, src)
-            mb.check(mb.lib().mosp_write_tree(os.path.join(tmp, f"d{k}.txt").encode(),
-                                              os.path.join(tmp, f"t{k}.txt").encode(), g.n, d.ctypes.data,
-                                              p.ctypes.data))
-        upd = mb.apply_batch(g, batch)
-        urow, ucol, uw = upd.arrays()
-        ch = mb.changed_lists(batch.arrays(), K)
+            d, p = orc.ref_dijkstra(row, col, w, k, src)
+            orc.ref_write_tree(os.path.join(tmp, f"d{k}.txt"), os.path.join(tmp, f"t{k}.txt"), d, p)
 
         def objective(k):
-            if have_ref:
-                ok = orc.ref_sequential_update(prefix, os.path.join(tmp, f"d{k}.txt"), os.path.join(tmp, f"t{k}.txt"),
-                                               ins, dele, k, src, os.path.join(tmp, f"od{k}.txt"),
-                                               os.path.join(tmp, f"ot{k}.txt"))
-                assert ok
-                p = np.empty(g.n, np.int32)
-                d = np.empty(g.n, np.int64)
-                mb.check(mb.lib().mosp_read_tree(os.path.join(tmp, f"od{k}.txt").encode(),
-                                                 os.path.join(tmp, f"ot{k}.txt").encode(), g.n, d.ctypes.data,
-                                                 p.ctypes.data))
-                return p
-            d0, p0 = orc.dijkstra(row, col, w, k, src)
-            return orc.sequential_update(urow, ucol, uw, k, src, ch[k][0], ch[k][1], ba["ins_to"], d0, p0)[1]
-
-        def one_step():
             t0 = time.perf_counter()
-            with ThreadPoolExecutor(max_workers=K) as pool:
-                parents = list(pool.map(objective, range(K)))
-            if have_ref:
-                orc.ref_combined_dijkstra(np.stack(parents), g.n, K, src, pref)
-            else:
-                crow, ccol, cw = orc.combined_graph(np.stack(parents), g.n, K, src, pref)
-                orc.dijkstra(crow, ccol, cw, 0, src)
-            return time.perf_counter() - t0
+            ok, compute = orc.ref_sequential_update_timed(prefix, os.path.join(tmp, f"d{k}.txt"),
+                                                          os.path.join(tmp, f"t{k}.txt"), ins, dele, k, src,
+                                                          os.path.join(tmp, f"od{k}.txt"),
+                                                          os.path.join(tmp, f"ot{k}.txt"))
+            whole = time.perf_counter() - t0
+            if not ok:
+                raise RuntimeError(f"the reference's sequentialSOSPUpdate failed on objective {k}")
+            return whole, compute
 
-        first = one_step()  # warm-up (file cache, page faults)
-        budget = 200.0
-        steps = max(1, min(args.steps, int(budget / max(first, 1e-3))))
-        times = [one_step() for _ in range(steps)]
-        secs = float(np.mean(times))
-        value = changed / secs
-        kind = "reference" if have_ref else "port"
-        sample = (("reference sequentialSOSPUpdate (file API, text read/write included, as the reference's CPU "
-                   f"path runs) per objective, K={K} objectives in parallel threads, then the reference "
-                   "combinedGraphReference + dijkstraCsrGraph") if have_ref else
-                  "oracle restatement of the reference CPU path (compute only)")
-        line = {"metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": steps,
-                "steps_requested": args.steps, "warmup": 1, "ms_per_step": round(secs * 1000, 2),
+        for i in range(max(args.warmup, 0)):
+            objective(i % K)
+        whole, compute = [], []
+        for i in range(max(args.steps, 1)):
+            a, b = objective(i % K)
+            whole.append(a)
+            compute.append(b)
+        for k in range(K):  # every objective's output tree exists
+            if not os.path.exists(os.path.join(tmp, f"ot{k}.txt")):
+                objective(k)
+        t0 = time.perf_counter()
+        parents = np.stack([orc.ref_read_parents(os.path.join(tmp, f"ot{k}.txt"), n) for k in range(K)])
+        t1 = time.perf_counter()
+        orc.ref_combined_dijkstra(parents, n, K, src, pref)
+        t2 = time.perf_counter()
+        comb_whole, comb_compute = t2 - t0, t2 - t1
+        per_update = K * float(np.mean(whole)) + comb_whole
+        per_update_compute = K * float(np.mean(compute)) + comb_compute
+        value = changed / per_update
+
+        # labelled variant, not the reference's behaviour: the K objectives
+        # in K threads at once (one update, after the timed steps)
+        from concurrent.futures import ThreadPoolExecutor
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(max_workers=K) as pool:
+            list(pool.map(objective, range(K)))
+        threaded = time.perf_counter() - t0 + comb_whole
+
+        cores = os.cpu_count() or 1
+        sample = (f"one objective's reference sequentialSOSPUpdate per step (file API: text graph, batch and tree "
+                  f"read, batch applied, update, tree written; objective = step mod {K}), then once the "
+                  f"reference's combinedGraphReference + dijkstraCsrGraph on the {K} written trees; one host "
+                  f"thread ({cores} cores on the host); value = changed edges / ({K} x mean step + combined)")
+        line = {"metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": len(whole),
+                "warmup": max(args.warmup, 0), "ms_per_step": round(1000 * float(np.mean(whole)), 2),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
                 "data": "synthetic", "impl": "reference",
-                "config": {"workload": workload, "n": g.n, "m": upd.m, "K": K, "changes_applied": changed,
-                           "parallelism": "CPU, one thread per objective"},
-                "cpu_baseline": {"value": round(value, 2), "unit": UNIT, "cores": K, "kind": kind,
-                                 "sample": sample + f"; full workload per step, {steps} timed step(s)"},
-                "e2e": {"value": round(value, 2), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                "config": shared_config(workload, n, m_upd, K, changed, n_ins, n_del),
+                "cpu_baseline": {"value": round(value, 2), "unit": UNIT, "cores": 1, "kind": "reference",
+                                 "sample": sample},
+                "e2e": {"value": round(value, 2), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                "per_update_s": {"file_api": round(per_update, 3), "compute_only": round(per_update_compute, 3),
+                                 "objective_file_api": round(float(np.mean(whole)), 3),
+                                 "objective_compute_only": round(float(np.mean(compute)), 3),
+                                 "combined_file_api": round(comb_whole, 3), "combined_compute": round(comb_compute, 3)},
+                "compute_only": {"value": round(changed / per_update_compute, 2), "unit": UNIT,
+                                 "what": "the reference's Phases 1-2 per objective (clock reads in a second copy of "
+                                         "its source) + combinedGraphReference + dijkstraCsrGraph"},
+                "threaded_variant": {"value": round(changed / threaded, 2), "unit": UNIT, "threads": K,
+                                     "what": f"not the reference's behaviour: the {K} objectives in {K} threads at "
+                                             "once, file API, plus the combined step"},
+                "host": {"cores": cores}}
         print(json.dumps(line), flush=True)
     finally:
         shutil.rmtree(tmp, ignore_errors=True)

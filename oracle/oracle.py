@@ -6,8 +6,12 @@
   code compiled from its sources (present only where the reference sources
   were available at build time; ``have_ref()`` says whether it is).
 
-Only tests/, __graft_entry__.smoke() and the cpu_baseline leg of bench.py
-use this module; the product never does.
+* ``workload_*`` functions build the seeded benchmark graphs from
+  oracle/_gen/libworkload.so (the library's generators compiled on their
+  own), for the benchmark's reference arm.
+
+Only tests/, __graft_entry__.smoke() and the cpu_baseline and reference
+legs of bench.py use this module; the product never does.
 """
 from __future__ import annotations
 
@@ -44,10 +48,23 @@ _REF_SIGS = {
     "ref_combined_dijkstra": (_i, [_i, _i, _p, _i, _p, _p, _p, _p]),
     "ref_path_costs": (_i, [_i, _i, _p, _p, _p, _p, _i, _p]),
     "ref_sequential_update": (_i, [C.c_char_p] * 5 + [_i, _i, C.c_char_p, C.c_char_p]),
+    "ref_sequential_update_timed": (_i, [C.c_char_p] * 5 + [_i, _i, C.c_char_p, C.c_char_p, _p]),
+    "ref_write_csr": (_i, [C.c_char_p, _i, _i, _p, _p, _p]),
+    "ref_write_changes": (_i, [C.c_char_p, C.c_char_p, _i, _i, _p, _p, _p, _i, _p, _p]),
+    "ref_write_tree": (_i, [C.c_char_p, C.c_char_p, _i, _p, _p]),
+    "ref_read_parents": (_i, [C.c_char_p, _i, _p]),
 }
+_WORKLOAD_SIGS = {
+    "wl_grid_road": (_p, [_i, _i, C.c_double, C.c_double, _i, _i, _i, C.c_uint, _p, _p]),
+    "wl_rmat": (_p, [_i, _i, C.c_double, C.c_double, C.c_double, _i, _i, _i, _i, C.c_uint, _p, _p]),
+    "wl_copy": (None, [_p, _p, _p, _p]),
+    "wl_free": (None, [_p]),
+}
+WORKLOAD_LIB = os.path.join(HERE, "_gen", "libworkload.so")
 
 _olib = None
 _rlib = None
+_wlib = None
 
 
 def _load(path, sigs):
@@ -75,6 +92,13 @@ def rlib():
     if _rlib is None:
         _rlib = _load(REF_LIB, _REF_SIGS)
     return _rlib
+
+
+def wlib():
+    global _wlib
+    if _wlib is None:
+        _wlib = _load(WORKLOAD_LIB, _WORKLOAD_SIGS)
+    return _wlib
 
 
 def _a(x, dt):
@@ -276,3 +300,71 @@ def ref_sequential_update(graph_prefix, dist_in, tree_in, insert_path, delete_pa
     e = lambda s: s.encode()  # noqa: E731
     return rlib().ref_sequential_update(e(graph_prefix), e(dist_in), e(tree_in), e(insert_path),
                                         e(delete_path), k, source, e(dist_out), e(tree_out)) == 0
+
+
+def ref_sequential_update_timed(graph_prefix, dist_in, tree_in, insert_path, delete_path, k, source, dist_out,
+                                tree_out):
+    """The same call through the instrumented copy: (ok, seconds of its
+    Phases 1-2, the update computation alone)."""
+    e = lambda s: s.encode()  # noqa: E731
+    secs = C.c_double()
+    rc = rlib().ref_sequential_update_timed(e(graph_prefix), e(dist_in), e(tree_in), e(insert_path),
+                                            e(delete_path), k, source, e(dist_out), e(tree_out),
+                                            C.addressof(secs))
+    return rc == 0, secs.value
+
+
+def ref_write_csr(prefix, row, col, w):
+    row, col, w = _a(row, np.int32), _a(col, np.int32), _a(w, np.int32)
+    if rlib().ref_write_csr(prefix.encode(), len(row) - 1, w.shape[1], P(row), P(col), P(w)) != 0:
+        raise OSError(f"ref_write_csr failed for {prefix}")
+
+
+def ref_write_changes(insert_path, delete_path, K, batch):
+    ifr, ito = _a(batch["ins_from"], np.int32), _a(batch["ins_to"], np.int32)
+    iw = _a(batch["ins_w"], np.int32)
+    dfr, dto = _a(batch["del_from"], np.int32), _a(batch["del_to"], np.int32)
+    if rlib().ref_write_changes(insert_path.encode(), delete_path.encode(), K, len(ifr), P(ifr), P(ito), P(iw),
+                                len(dfr), P(dfr), P(dto)) != 0:
+        raise OSError("ref_write_changes failed")
+
+
+def ref_write_tree(dist_path, tree_path, dist, parent):
+    d, p = _a(dist, np.int64), _a(parent, np.int32)
+    if rlib().ref_write_tree(dist_path.encode(), tree_path.encode(), len(d), P(d), P(p)) != 0:
+        raise OSError("ref_write_tree failed")
+
+
+def ref_read_parents(path, n):
+    p = np.empty(n, np.int32)
+    if rlib().ref_read_parents(path.encode(), n, P(p)) != 0:
+        raise OSError(f"ref_read_parents failed for {path}")
+    return p
+
+
+# ---------------------------------------------------------------------------
+# Seeded benchmark graphs (oracle/_gen/libworkload.so: the library's own
+# generators, built without the library)
+# ---------------------------------------------------------------------------
+def _workload(handle, n, m, K):
+    if not handle:
+        raise ValueError("invalid workload parameters")
+    row = np.empty(n.value + 1, np.int32)
+    col = np.empty(max(m.value, 1), np.int32)
+    w = np.empty((max(m.value, 1), K), np.int32)
+    wlib().wl_copy(handle, P(row), P(col), P(w))
+    wlib().wl_free(handle)
+    return row, col[: m.value], w[: m.value]
+
+
+def workload_grid_road(width, height, keep, shortcut, K, wmin, wmax, seed):
+    n, m = C.c_int(), C.c_longlong()
+    h = wlib().wl_grid_road(width, height, keep, shortcut, K, wmin, wmax, seed, C.addressof(n), C.addressof(m))
+    return _workload(h, n, m, K)
+
+
+def workload_rmat(scale, edge_factor, a, b, c, K, wmin, wmax, log_uniform, seed):
+    n, m = C.c_int(), C.c_longlong()
+    h = wlib().wl_rmat(scale, edge_factor, a, b, c, K, wmin, wmax, int(log_uniform), seed, C.addressof(n),
+                       C.addressof(m))
+    return _workload(h, n, m, K)

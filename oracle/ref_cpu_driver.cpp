@@ -13,11 +13,22 @@
 #include "validation.cuh"
 
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <string>
 #include <vector>
 
+// The compute-only variant of the sequential update: the same source
+// compiled a second time under another name, with a clock read inserted at
+// the start of its Phase 1 and at the start of its output stage
+// (oracle/instrument_ref.py writes that copy into _ref/ at build time).
+bool sequentialSOSPUpdateTimed(const std::string &, const std::string &, const std::string &,
+                               const std::string &, const std::string &, int, int,
+                               const std::string &, const std::string &);
+
 namespace {
+
+std::chrono::steady_clock::time_point g_marks[3];
 
 CsrGraph makeGraph(int n, int K, const int *row, const int *col, const int *w) {
   CsrGraph g;
@@ -120,6 +131,46 @@ int ref_path_costs(int n, int KG, const int *row, const int *col, const int *w, 
   return 0;
 }
 
+/// Clock read of the instrumented copy: 1 = Phase 1 starts (input read and
+/// batch applied), 2 = output stage starts (update computed).
+void mosp_ref_phase_mark(int which) {
+  if (which >= 0 && which < 3) g_marks[which] = std::chrono::steady_clock::now();
+}
+
+/// The reference's own text writers and reader (the formats its CPU path
+/// reads and writes), so that the benchmark's reference arm needs no other
+/// library for its input and output files.
+int ref_write_csr(const char *prefix, int n, int K, const int *row, const int *col, const int *w) {
+  return writeCsrGraph(prefix, makeGraph(n, K, row, col, w)) ? 0 : -1;
+}
+
+int ref_write_changes(const char *insert_path, const char *delete_path, int K, int n_ins,
+                      const int *ins_from, const int *ins_to, const int *ins_w, int n_del,
+                      const int *del_from, const int *del_to) {
+  ChangeBatch b;
+  b.numberOfObjectives = K;
+  b.insertFrom.assign(ins_from, ins_from + n_ins);
+  b.insertTo.assign(ins_to, ins_to + n_ins);
+  b.insertWeights.assign(ins_w, ins_w + static_cast<size_t>(n_ins) * K);
+  b.deleteFrom.assign(del_from, del_from + n_del);
+  b.deleteTo.assign(del_to, del_to + n_del);
+  return writeChangeBatch(b, insert_path, delete_path) ? 0 : -1;
+}
+
+int ref_write_tree(const char *dist_path, const char *tree_path, int n, const long long *dist,
+                   const int *parent) {
+  const bool ok = writeDistances(dist_path, std::vector<long long>(dist, dist + n)) &&
+                  writeParents(tree_path, std::vector<int>(parent, parent + n));
+  return ok ? 0 : -1;
+}
+
+int ref_read_parents(const char *path, int n, int *parent) {
+  std::vector<int> p;
+  if (!readParents(path, n, p)) return -1;
+  std::copy(p.begin(), p.end(), parent);
+  return 0;
+}
+
 /// The reference's CPU update path as its tests call it (file API).
 int ref_sequential_update(const char *graph_prefix, const char *dist_in, const char *tree_in,
                           const char *insert_path, const char *delete_path, int objective,
@@ -128,6 +179,22 @@ int ref_sequential_update(const char *graph_prefix, const char *dist_in, const c
                               source, dist_out, tree_out)
              ? 0
              : -1;
+}
+
+/// The same update, from the instrumented copy: *compute_s receives the
+/// time of its Phases 1-2 (roots, subtree invalidation, relaxation), without
+/// the text input, the batch application and the output.
+int ref_sequential_update_timed(const char *graph_prefix, const char *dist_in, const char *tree_in,
+                                const char *insert_path, const char *delete_path, int objective,
+                                int source, const char *dist_out, const char *tree_out,
+                                double *compute_s) {
+  g_marks[1] = g_marks[2] = std::chrono::steady_clock::time_point();
+  const bool ok = sequentialSOSPUpdateTimed(graph_prefix, dist_in, tree_in, insert_path, delete_path,
+                                            objective, source, dist_out, tree_out);
+  if (compute_s != nullptr) {
+    *compute_s = std::chrono::duration<double>(g_marks[2] - g_marks[1]).count();
+  }
+  return ok ? 0 : -1;
 }
 
 }  // extern "C"

@@ -45,3 +45,47 @@ def test_powerlaw_full_size_takes_the_fallback():
     assert mb.choose_packing(1 << 22, 1_000_000)[0] == 0
     assert mb.choose_packing(1 << 20, 10_000_000)[0] == 0
     assert mb.choose_packing(1 << 20, 1_000_000)[0] > 0
+
+
+def test_reference_arm_builds_the_same_workload():
+    """The reference arm builds its input from oracle/ alone (the standalone
+    generator library and the reference's own change generator); graph and
+    batch equal the library arm's, for both configurations."""
+    import numpy as np
+    import oracle as orc
+    if not orc.have_ref():
+        import pytest
+        pytest.skip("oracle/_ref not built")
+    for a in (args(), args(workload="powerlaw", rmat_scale=10, rmat_wmax=10_000_000)):
+        g, b, K, pref, desc = bench.make_workload(a)
+        row, col, w, batch, K2, pref2, desc2 = bench.reference_workload(a)
+        grow, gcol, gw = g.arrays()
+        assert np.array_equal(row, grow) and np.array_equal(col, gcol) and np.array_equal(w, gw)
+        ba = b.arrays()
+        for key in ("ins_from", "ins_to", "ins_w", "del_from", "del_to"):
+            assert np.array_equal(np.asarray(batch[key]).reshape(np.asarray(ba[key]).shape), ba[key]), key
+        assert (K2, pref2, desc2) == (K, pref, desc)
+
+
+def test_reference_arm_loads_no_library_code():
+    """`bench.py --impl reference` maps only oracle/ libraries: none of this
+    library's shared objects is loaded in its process."""
+    import os
+    import subprocess
+    import sys
+    import oracle as orc
+    if not orc.have_ref():
+        import pytest
+        pytest.skip("oracle/_ref not built")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = ("import sys, argparse, bench\n"
+            "a = argparse.Namespace(workload='road', width=40, changes=200, rmat_scale=22, rmat_wmax=10**6, "
+            "steps=3, warmup=1, gpus=1)\n"
+            "bench.run_reference(a)\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "print('LIBRARY_MAPPED' if 'libmosp_b200' in maps else 'CLEAN', 'mosp_b200' in sys.modules)\n")
+    out = subprocess.run([sys.executable, "-c", code], cwd=root, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr[-2000:]
+    last = out.stdout.strip().splitlines()[-1]
+    assert last == "CLEAN False", last
+    assert '"impl": "reference"' in out.stdout
