@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <queue>
 #include <sstream>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -57,51 +58,82 @@ bool runDijkstraCSR(const std::string &inputPrefix, int objectiveNumber, int sou
 
 std::string TreeCheck::summary() const {
   std::ostringstream out;
-  out << "distance mismatches=" << distanceMismatches
-      << " inconsistent parents=" << inconsistentParents
-      << " non-canonical parents=" << nonCanonicalParents
-      << " parent mismatches=" << parentMismatches;
+  out << "distances off: " << distanceMismatches << ", parents not on a tight edge: "
+      << inconsistentParents << ", tight but not the lowest id: " << nonCanonicalParents
+      << ", parents unlike the reference: " << parentMismatches;
   return out.str();
 }
+
+namespace {
+
+/// The four counts of TreeCheck for the vertices [lo, hi).
+struct RangeVerdict {
+  long long distance = 0, inconsistent = 0, nonCanonical = 0, mismatch = 0;
+};
+
+bool reachable(long long d) { return d < DISTANCE_INF / 2; }
+
+/// Lowest in-neighbour u of v with d[u] + w(u, v) == d[v] (-1 if none), and
+/// whether `p` is one of them.
+std::pair<int, bool> tightParents(const CsrGraph &reverse, int objective,
+                                  const std::vector<long long> &d, int v, int p) {
+  int lowest = -1;
+  bool pTight = false;
+  for (int e = reverse.rowPtr[v]; e < reverse.rowPtr[v + 1]; ++e) {
+    const int u = reverse.colInd[e];
+    if (!reachable(d[u]) || d[u] + reverse.weight(e, objective) != d[v]) continue;
+    lowest = lowest < 0 ? u : std::min(lowest, u);
+    pTight = pTight || u == p;
+  }
+  return {lowest, pTight};
+}
+
+}  // namespace
 
 TreeCheck checkSospTree(const CsrGraph &reverse, int objective, int source,
                         const std::vector<long long> &distances, const std::vector<int> &parents,
                         const std::vector<long long> &referenceDistances,
                         const std::vector<int> *referenceParents) {
-  TreeCheck check;
   const int n = reverse.numberOfNodes;
-  auto finite = [](long long d) { return d < DISTANCE_INF / 2; };
-  for (int v = 0; v < n; ++v) {
-    const long long dv = distances[v];
-    const bool reach = finite(dv);
-    if (reach != finite(referenceDistances[v]) || (reach && dv != referenceDistances[v])) {
-      ++check.distanceMismatches;
+  auto judge = [&](int lo, int hi) {
+    RangeVerdict r;
+    for (int v = lo; v < hi; ++v) {
+      const long long dv = distances[v], rv = referenceDistances[v];
+      if (reachable(dv) != reachable(rv) || (reachable(dv) && dv != rv)) ++r.distance;
+      if (referenceParents != nullptr && parents[v] != (*referenceParents)[v]) ++r.mismatch;
+      const int p = parents[v];
+      if (v == source || !reachable(dv)) {
+        // the source (distance 0) and unreachable vertices have no parent
+        if (p != -1 || (v == source && dv != 0)) ++r.inconsistent;
+        continue;
+      }
+      const auto [lowest, pTight] = tightParents(reverse, objective, distances, v, p);
+      if (!pTight) {
+        ++r.inconsistent;
+      } else if (p != lowest) {
+        ++r.nonCanonical;
+      }
     }
-    if (referenceParents != nullptr && parents[v] != (*referenceParents)[v]) {
-      ++check.parentMismatches;
-    }
-    if (v == source) {
-      if (parents[v] != -1 || dv != 0) ++check.inconsistentParents;
-      continue;
-    }
-    if (!reach) {
-      if (parents[v] != -1) ++check.inconsistentParents;
-      continue;
-    }
-    const int p = parents[v];
-    bool tight = false;
-    int lowest = -1;
-    for (int e = reverse.rowPtr[v]; e < reverse.rowPtr[v + 1]; ++e) {
-      const int u = reverse.colInd[e];
-      if (!finite(distances[u]) || distances[u] + reverse.weight(e, objective) != dv) continue;
-      if (u == p) tight = true;
-      if (lowest < 0 || u < lowest) lowest = u;
-    }
-    if (!tight) {
-      ++check.inconsistentParents;
-    } else if (p != lowest) {
-      ++check.nonCanonicalParents;
-    }
+    return r;
+  };
+  // vertex ranges checked side by side; every range's counts are summed
+  const int workers = std::max(1, std::min<int>(std::thread::hardware_concurrency(), n / 65536 + 1));
+  std::vector<RangeVerdict> part(workers);
+  std::vector<std::thread> pool;
+  for (int t = 1; t < workers; ++t) {
+    pool.emplace_back([&, t] {
+      part[t] = judge(static_cast<int>(static_cast<long long>(n) * t / workers),
+                      static_cast<int>(static_cast<long long>(n) * (t + 1) / workers));
+    });
+  }
+  part[0] = judge(0, static_cast<int>(static_cast<long long>(n) / workers));
+  for (std::thread &th : pool) th.join();
+  TreeCheck check;
+  for (const RangeVerdict &r : part) {
+    check.distanceMismatches += r.distance;
+    check.inconsistentParents += r.inconsistent;
+    check.nonCanonicalParents += r.nonCanonical;
+    check.parentMismatches += r.mismatch;
   }
   return check;
 }

@@ -13,6 +13,7 @@
 // the objective values of the MOSP path to v, every objective of the graph).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <charconv>
 #include <chrono>
 #include <climits>
@@ -23,6 +24,7 @@
 #include <iostream>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "csrGraph.cuh"
@@ -51,66 +53,86 @@ void usage() {
                "            [--quiet]\n";
 }
 
+/// One command-line flag: how many values it takes and what it does with
+/// its value (a false return is a usage error).
+struct Flag {
+  const char *name;
+  bool takesValue;
+  std::function<bool(Options &, const std::string &)> apply;
+};
+
+bool intInRange(const std::string &flag, const std::string &text, long long lo, long long hi,
+                long long &out) {
+  if (parseInteger(text, lo, hi, out)) return true;
+  std::cerr << flag << ": expected an integer from " << lo << " to " << hi << ", not '" << text
+            << "'\n";
+  return false;
+}
+
+const std::vector<Flag> &flagTable() {
+  static const std::vector<Flag> table = {
+      {"--graph", true, [](Options &o, const std::string &v) { o.graph = v; return true; }},
+      {"--changes", true, [](Options &o, const std::string &v) { o.changes = v; return true; }},
+      {"--init", true, [](Options &o, const std::string &v) { o.init = v; return true; }},
+      {"--out", true, [](Options &o, const std::string &v) { o.out = v; return true; }},
+      {"--timing", true, [](Options &o, const std::string &v) { o.timingCsv = v; return true; }},
+      {"--cache", true, [](Options &o, const std::string &v) { o.cache = v; return true; }},
+      {"-k", true,
+       [](Options &o, const std::string &v) {
+         long long x = 0;
+         if (!intInRange("-k", v, 0, INT_MAX, x)) return false;
+         o.K = static_cast<int>(x);
+         return true;
+       }},
+      {"--source", true,
+       [](Options &o, const std::string &v) {
+         long long x = 0;
+         if (!intInRange("--source", v, 0, INT_MAX, x)) return false;
+         o.source = static_cast<int>(x);
+         return true;
+       }},
+      {"--delta", true,
+       [](Options &o, const std::string &v) { return intInRange("--delta", v, 1, LLONG_MAX, o.delta); }},
+      {"--pref", true,
+       [](Options &o, const std::string &v) {
+         // comma-separated preference weights, each >= 1
+         size_t from = 0;
+         while (from < v.size()) {
+           const size_t comma = std::min(v.find(',', from), v.size());
+           long long x = 0;
+           if (!intInRange("--pref", v.substr(from, comma - from), 1, INT_MAX, x)) return false;
+           o.pref.push_back(static_cast<int>(x));
+           from = comma + 1;
+         }
+         return true;
+       }},
+      {"--canonicalize", false, [](Options &o, const std::string &) { return o.canonicalize = true; }},
+      {"--no-output", false, [](Options &o, const std::string &) { o.writeOutput = false; return true; }},
+      {"--validate", false, [](Options &o, const std::string &) { return o.validate = true; }},
+      {"--quiet", false, [](Options &o, const std::string &) { return o.quiet = true; }},
+  };
+  return table;
+}
+
 bool parseOptions(int argc, char **argv, Options &o) {
+  const std::vector<Flag> &table = flagTable();
   for (int i = 1; i < argc; ++i) {
-    const std::string a = argv[i];
-    auto next = [&](std::string &dst) {
-      if (i + 1 >= argc) return false;
-      dst = argv[++i];
-      return true;
-    };
-    std::string v;
-    long long x = 0;
-    auto integer = [&](long long lo, long long hi) {
-      if (!next(v)) return false;
-      if (parseInteger(v, lo, hi, x)) return true;
-      std::cerr << a << " needs an integer in [" << lo << ", " << hi << "], got '" << v << "'\n";
-      return false;
-    };
-    if (a == "--graph") {
-      if (!next(o.graph)) return false;
-    } else if (a == "--changes") {
-      if (!next(o.changes)) return false;
-    } else if (a == "--init") {
-      if (!next(o.init)) return false;
-    } else if (a == "--out") {
-      if (!next(o.out)) return false;
-    } else if (a == "--timing") {
-      if (!next(o.timingCsv)) return false;
-    } else if (a == "--cache") {
-      if (!next(o.cache)) return false;
-    } else if (a == "-k") {
-      if (!integer(0, INT_MAX)) return false;
-      o.K = static_cast<int>(x);
-    } else if (a == "--source") {
-      if (!integer(0, INT_MAX)) return false;
-      o.source = static_cast<int>(x);
-    } else if (a == "--delta") {
-      if (!integer(1, LLONG_MAX)) return false;
-      o.delta = x;
-    } else if (a == "--pref") {
-      if (!next(v)) return false;
-      std::istringstream list(v);
-      std::string item;
-      while (std::getline(list, item, ',')) {
-        if (!parseInteger(item, 1, INT_MAX, x)) {
-          std::cerr << "--pref needs integers >= 1, got '" << v << "'\n";
-          return false;
-        }
-        o.pref.push_back(static_cast<int>(x));
-      }
-    } else if (a == "--canonicalize") {
-      o.canonicalize = true;
-    } else if (a == "--no-output") {
-      o.writeOutput = false;
-    } else if (a == "--validate") {
-      o.validate = true;
-    } else if (a == "--quiet") {
-      o.quiet = true;
-    } else {
-      std::cerr << "unknown option: " << a << "\n";
+    const std::string arg = argv[i];
+    const auto flag = std::find_if(table.begin(), table.end(),
+                                   [&](const Flag &f) { return arg == f.name; });
+    if (flag == table.end()) {
+      std::cerr << "mosp: no such option: " << arg << "\n";
       return false;
     }
+    std::string value;
+    if (flag->takesValue) {
+      if (i + 1 == argc) {
+        std::cerr << "mosp: " << arg << " needs a value\n";
+        return false;
+      }
+      value = argv[++i];
+    }
+    if (!flag->apply(o, value)) return false;
   }
   return !o.graph.empty() && !o.changes.empty() && !o.init.empty();
 }
@@ -119,10 +141,11 @@ double msSince(std::chrono::steady_clock::time_point t) {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
 }
 
+/// Objective k's part of a K * n objective-major array.
 template <typename T>
-std::vector<T> slice(const std::vector<T> &all, int k, int n) {
-  return std::vector<T>(all.begin() + static_cast<size_t>(k) * n,
-                        all.begin() + static_cast<size_t>(k + 1) * n);
+std::vector<T> objectivePart(const std::vector<T> &all, int k, int n) {
+  const auto first = all.begin() + static_cast<std::ptrdiff_t>(k) * n;
+  return std::vector<T>(first, first + n);
 }
 
 bool writeCosts(const std::string &path, const std::vector<long long> &costs, int KG) {
@@ -143,34 +166,48 @@ bool writeCosts(const std::string &path, const std::vector<long long> &costs, in
   });
 }
 
+/// --validate: every updated tree against host Dijkstra on the updated
+/// graph (exact parents when the input trees were canonical), and the MOSP
+/// tree against Dijkstra on the host combined graph of the updated trees.
+/// The K + 1 checks are independent and run side by side; the report lines
+/// come out in objective order.
 bool validate(const CsrGraph &updated, const MospResult &r, int source, const std::vector<int> &pref,
               bool requireCanonical) {
   const int n = updated.numberOfNodes, K = r.numberOfObjectives;
   CsrGraph reverse;
   transposeCsrGraph(updated, reverse);
-  bool all = true;
-  for (int k = 0; k < K; ++k) {
+  std::vector<TreeCheck> checks(K + 1);
+  auto checkObjective = [&](int k) {
     std::vector<long long> refDist;
     std::vector<int> refParent;
     dijkstraCsrGraph(updated, k, source, refDist, refParent);
-    const TreeCheck c = checkSospTree(reverse, k, source, slice(r.distances, k, n),
-                                      slice(r.parents, k, n), refDist,
-                                      requireCanonical ? &refParent : nullptr);
-    const bool ok = c.ok(requireCanonical);
+    checks[k] = checkSospTree(reverse, k, source, objectivePart(r.distances, k, n),
+                              objectivePart(r.parents, k, n), refDist,
+                              requireCanonical ? &refParent : nullptr);
+  };
+  auto checkCombined = [&] {
+    const CsrGraph combined = combinedGraphReference(r.parents, n, K, source, pref);
+    CsrGraph combinedReverse;
+    transposeCsrGraph(combined, combinedReverse);
+    std::vector<long long> refDist;
+    std::vector<int> refParent;
+    dijkstraCsrGraph(combined, 0, source, refDist, refParent);
+    checks[K] = checkSospTree(combinedReverse, 0, source, r.combinedDistances, r.combinedParent,
+                              refDist, &refParent);
+  };
+  std::vector<std::thread> workers;
+  for (int k = 0; k < K; ++k) workers.emplace_back(checkObjective, k);
+  checkCombined();
+  for (std::thread &t : workers) t.join();
+  bool all = true;
+  for (int k = 0; k <= K; ++k) {
+    // the MOSP tree is computed from scratch, so it is always canonical
+    const bool ok = checks[k].ok(k == K || requireCanonical);
     all = all && ok;
-    std::cout << "VALIDATE obj" << k << " " << (ok ? "PASS" : "FAIL") << " (" << c.summary() << ")\n";
+    std::cout << "VALIDATE " << (k == K ? std::string("combined") : "obj" + std::to_string(k)) << " "
+              << (ok ? "PASS" : "FAIL") << " (" << checks[k].summary() << ")\n";
   }
-  const CsrGraph combined = combinedGraphReference(r.parents, n, K, source, pref);
-  CsrGraph combinedReverse;
-  transposeCsrGraph(combined, combinedReverse);
-  std::vector<long long> refDist;
-  std::vector<int> refParent;
-  dijkstraCsrGraph(combined, 0, source, refDist, refParent);
-  const TreeCheck c = checkSospTree(combinedReverse, 0, source, r.combinedDistances,
-                                    r.combinedParent, refDist, &refParent);
-  const bool ok = c.ok(true);  // built from scratch: always canonical
-  std::cout << "VALIDATE combined " << (ok ? "PASS" : "FAIL") << " (" << c.summary() << ")\n";
-  return all && ok;
+  return all;
 }
 
 }  // namespace
@@ -226,7 +263,7 @@ int main(int argc, char **argv) {
   if (opt.canonicalize) {
     const auto tc = std::chrono::steady_clock::now();
     for (int k = 0; k < K; ++k) {
-      canonicalizeTree(original, k, opt.source, slice(distances, k, n),
+      canonicalizeTree(original, k, opt.source, objectivePart(distances, k, n),
                        parents.data() + static_cast<size_t>(k) * n);
     }
     canonicalizeMs = msSince(tc);
@@ -254,10 +291,10 @@ int main(int argc, char **argv) {
     for (int k = 0; k < K; ++k) {
       const std::string dir = opt.out + "/obj" + std::to_string(k);
       writes.push_back([&, k, dir] {
-        return writeDistances(dir + "/distancesUpdated.txt", slice(result.distances, k, n));
+        return writeDistances(dir + "/distancesUpdated.txt", objectivePart(result.distances, k, n));
       });
       writes.push_back([&, k, dir] {
-        return writeParents(dir + "/SSSPTreeUpdated.txt", slice(result.parents, k, n));
+        return writeParents(dir + "/SSSPTreeUpdated.txt", objectivePart(result.parents, k, n));
       });
     }
     const std::string comb = opt.out + "/combinedGraph";

@@ -19,15 +19,19 @@
 // --gpu computes the trees with the canonical SSSP engine on the GPU
 // instead of host Dijkstra (identical output).
 #include <algorithm>
+#include <charconv>
 #include <chrono>
 #include <climits>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <fstream>
 #include <iostream>
+#include <iterator>
 #include <random>
 #include <string>
+#include <string_view>
 #include <vector>
 
 #include "changeGenerator.cuh"
@@ -87,85 +91,118 @@ bool parseReal(const char *text, double lo, double hi, double &x) {
   return end != text && *end == '\0' && x >= lo && x <= hi;
 }
 
-/// Matrix Market -> CSR text: symmetric files give both directions,
-/// self-loops and duplicates are dropped, K uniform weights per edge.
+/// Next line of `text` from `pos` (without its newline); false at the end.
+bool nextLine(const std::string &text, size_t &pos, std::string_view &line) {
+  if (pos >= text.size()) return false;
+  const size_t eol = std::min(text.find('\n', pos), text.size());
+  line = std::string_view(text).substr(pos, eol - pos);
+  pos = eol + 1;
+  return true;
+}
+
+/// Leading integers of a line (blanks between), at most `want` of them.
+int leadingIntegers(std::string_view line, long long *out, int want) {
+  int got = 0;
+  const char *p = line.data(), *end = line.data() + line.size();
+  while (got < want) {
+    while (p < end && (*p == ' ' || *p == '\t' || *p == '\r')) ++p;
+    const auto r = std::from_chars(p, end, out[got]);
+    if (r.ec != std::errc()) break;
+    p = r.ptr;
+    ++got;
+  }
+  return got;
+}
+
+/// Matrix Market -> CSR text: a "symmetric" file gives both directions,
+/// self-loops and repeated pairs are dropped, every edge gets K weights
+/// uniform in [wmin, wmax] drawn edge by edge from mt19937(seed), the draw
+/// order the reference's mospPrep uses, so the same seed gives the same
+/// files.
 int mtxToCsr(const std::string &in, const std::string &prefix, int K, int wmin, int wmax,
              unsigned seed) {
-  FILE *f = std::fopen(in.c_str(), "r");
-  if (f == nullptr) {
-    std::perror(in.c_str());
+  std::ifstream file(in, std::ios::binary);
+  if (!file) {
+    std::cerr << in << ": cannot open\n";
     return 1;
   }
-  static char line[1 << 16];
-  if (std::fgets(line, sizeof(line), f) == nullptr) {
-    std::fclose(f);
+  const std::string text((std::istreambuf_iterator<char>(file)), std::istreambuf_iterator<char>());
+  size_t pos = 0;
+  std::string_view line;
+  if (!nextLine(text, pos, line)) {
+    std::cerr << in << ": empty file\n";
     return 1;
   }
-  const bool symmetric = std::strstr(line, "symmetric") != nullptr;
-  while (std::fgets(line, sizeof(line), f) != nullptr && line[0] == '%') {
-  }
-  long long rows = 0, cols = 0, entries = 0;
-  if (std::sscanf(line, "%lld %lld %lld", &rows, &cols, &entries) != 3 || rows <= 0 ||
-      rows != cols || rows > INT32_MAX) {
-    std::cerr << "invalid Matrix Market header\n";
-    std::fclose(f);
+  const bool symmetric = line.find("symmetric") != std::string_view::npos;
+  do {
+    if (!nextLine(text, pos, line)) line = std::string_view();
+  } while (!line.empty() && line.front() == '%');
+  long long size[3] = {0, 0, 0};
+  if (leadingIntegers(line, size, 3) != 3 || size[0] <= 0 || size[0] != size[1] ||
+      size[0] > INT32_MAX) {
+    std::cerr << in << ": the size line is not 'n n entries' for a square matrix\n";
     return 1;
   }
-  std::vector<uint64_t> keys;
-  keys.reserve(static_cast<size_t>(symmetric ? 2 * entries : entries));
+  const long long n = size[0], entries = size[2];
+  std::vector<uint64_t> pairs;
+  pairs.reserve(static_cast<size_t>(symmetric ? 2 * entries : entries));
   for (long long i = 0; i < entries; ++i) {
-    if (std::fgets(line, sizeof(line), f) == nullptr) {
-      std::cerr << "Matrix Market file ends after " << i << " of " << entries << " entries\n";
-      std::fclose(f);
+    if (!nextLine(text, pos, line)) {
+      std::cerr << in << ": " << entries << " entries announced, " << i << " found\n";
       return 1;
     }
-    char *p = line;
-    const long long a = std::strtoll(p, &p, 10) - 1;
-    const long long b = std::strtoll(p, &p, 10) - 1;
-    if (a == b || a < 0 || b < 0 || a >= rows || b >= rows) continue;
-    keys.push_back((static_cast<uint64_t>(a) << 32) | static_cast<uint32_t>(b));
-    if (symmetric) keys.push_back((static_cast<uint64_t>(b) << 32) | static_cast<uint32_t>(a));
+    long long ab[2] = {0, 0};
+    leadingIntegers(line, ab, 2);
+    const long long a = ab[0] - 1, b = ab[1] - 1;  // 1-based in the file
+    if (a < 0 || b < 0 || a >= n || b >= n || a == b) continue;
+    pairs.push_back(static_cast<uint64_t>(a) << 32 | static_cast<uint32_t>(b));
+    if (symmetric) pairs.push_back(static_cast<uint64_t>(b) << 32 | static_cast<uint32_t>(a));
   }
-  std::fclose(f);
-  std::sort(keys.begin(), keys.end());
-  keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+  std::sort(pairs.begin(), pairs.end());
+  pairs.erase(std::unique(pairs.begin(), pairs.end()), pairs.end());
   CsrGraph g;
-  g.numberOfNodes = static_cast<int>(rows);
+  g.numberOfNodes = static_cast<int>(n);
   g.numberOfObjectives = K;
-  g.rowPtr.assign(static_cast<size_t>(g.numberOfNodes) + 1, 0);
-  g.colInd.resize(keys.size());
-  for (size_t e = 0; e < keys.size(); ++e) {
-    ++g.rowPtr[(keys[e] >> 32) + 1];
-    g.colInd[e] = static_cast<int>(keys[e] & 0xffffffffu);
+  g.rowPtr.resize(static_cast<size_t>(n) + 1);
+  g.colInd.resize(pairs.size());
+  size_t e = 0;
+  for (int u = 0; u < g.numberOfNodes; ++u) {
+    g.rowPtr[u] = static_cast<int>(e);
+    for (; e < pairs.size() && (pairs[e] >> 32) == static_cast<uint64_t>(u); ++e) {
+      g.colInd[e] = static_cast<int>(pairs[e] & 0xffffffffu);
+    }
   }
-  for (int u = 0; u < g.numberOfNodes; ++u) g.rowPtr[u + 1] += g.rowPtr[u];
+  g.rowPtr[g.numberOfNodes] = static_cast<int>(e);
   std::mt19937 rng(seed);
-  std::uniform_int_distribution<int> weight(wmin, wmax);
-  g.weights.resize(keys.size() * K);
-  for (int &w : g.weights) w = weight(rng);
+  std::uniform_int_distribution<int> draw(wmin, wmax);
+  g.weights.resize(pairs.size() * static_cast<size_t>(K));
+  std::generate(g.weights.begin(), g.weights.end(), [&] { return draw(rng); });
   if (!writeCsrGraph(prefix, g)) return 1;
   std::cout << "mtx2csr: n=" << g.numberOfNodes << " directed edges=" << g.numberOfEdges()
             << " symmetric=" << symmetric << "\n";
   return 0;
 }
 
+/// More objectives for a CSR graph: the existing weights stay, each edge
+/// gets K - K_old new ones drawn from mt19937(seed), edge by edge.
 int widen(const std::string &in, const std::string &out, int K, int wmin, int wmax, unsigned seed) {
   CsrGraph g;
   if (!readCsrGraph(in, g)) return 1;
-  const int oldK = g.numberOfObjectives;
-  if (K < oldK) {
-    std::cerr << "graph already has " << oldK << " objectives\n";
+  const int had = g.numberOfObjectives;
+  if (K < had) {
+    std::cerr << in << " has " << had << " objectives already; widen only adds\n";
     return 1;
   }
   std::mt19937 rng(seed);
-  std::uniform_int_distribution<int> weight(wmin, wmax);
-  std::vector<int> w(static_cast<size_t>(g.numberOfEdges()) * K);
-  for (int e = 0; e < g.numberOfEdges(); ++e) {
-    for (int k = 0; k < K; ++k) {
-      w[static_cast<size_t>(e) * K + k] = k < oldK ? g.weight(e, k) : weight(rng);
-    }
+  std::uniform_int_distribution<int> draw(wmin, wmax);
+  const size_t m = static_cast<size_t>(g.numberOfEdges());
+  std::vector<int> wide(m * K);
+  for (size_t e = 0; e < m; ++e) {
+    int *dst = wide.data() + e * K;
+    std::copy_n(g.weights.data() + e * had, had, dst);
+    std::generate_n(dst + had, K - had, [&] { return draw(rng); });
   }
-  g.weights.swap(w);
+  g.weights = std::move(wide);
   g.numberOfObjectives = K;
   return writeCsrGraph(out, g) ? 0 : 1;
 }
