@@ -118,3 +118,80 @@ def test_static_calls_take_no_device_memory(ws):
     torch.cuda.synchronize()
     free_after, _ = torch.cuda.mem_get_info()
     assert free_after == free_before
+
+
+def test_static_distance_only_words(ws):
+    """A declared weight bound so large that (n - 1) * max_weight does not
+    fit next to the parent field (within the static limits no int32 weight
+    gets there): distance-only words and the in-launch lowest-id parent
+    recovery, through the static scratch, with tied distances."""
+    row, col, w = grid_graph(60, 60, 1, 4, 0.1, 26)
+    g, dg = upload(ws, row, col, w)
+    bound = 10 ** 12
+    for _ in range(2):
+        ds, ps, st = static_tree(g, dg, 5, 3, bound)
+        assert st.packed_parents == 0
+        dw, pw, _ = workspace_tree(ws, g, dg, 5, 3, bound)
+        assert np.array_equal(ds, dw) and np.array_equal(ps, pw)
+    de, pe = orc.dijkstra(row, col, w, 0, 5)
+    assert np.array_equal(ds, de) and np.array_equal(ps, pe)
+
+
+def test_static_hub_row(ws):
+    """A star hub of 3,000 edges (more than the 2,048 a warp expands alone):
+    the CTA-wide hub queue runs on the static scratch too."""
+    n = 6000
+    rng = np.random.default_rng(27)
+    edges = {(i, i + 1) for i in range(n - 1)} | {(0, v) for v in range(2, 3002)}
+    while len(edges) < n - 1 + 3000 + 6000:
+        u, v = rng.integers(0, n, 2)
+        if u != v:
+            edges.add((int(u), int(v)))
+    edges = sorted(edges)
+    row = np.zeros(n + 1, np.int32)
+    for u, _ in edges:
+        row[u + 1] += 1
+    row = np.cumsum(row).astype(np.int32)
+    col = np.array([v for _, v in edges], np.int32)
+    w = rng.integers(1, 500, (len(edges), 1)).astype(np.int32)
+    assert row[1] - row[0] > 2048
+    g, dg = upload(ws, row, col, w)
+    for _ in range(2):
+        ds, ps, _ = static_tree(g, dg, 0, 100, int(w.max()))
+        dw, pw, _ = workspace_tree(ws, g, dg, 0, 100, int(w.max()))
+        assert np.array_equal(ds, dw) and np.array_equal(ps, pw)
+    de, pe = orc.dijkstra(row, col, w, 0, 0)
+    assert np.array_equal(ds, de) and np.array_equal(ps, pe)
+
+
+def test_static_rejects_malformed_csr(ws):
+    """A CSR whose last offset exceeds the edge count, or with a column out
+    of range, is rejected on the device before any relaxation (small graph,
+    so even an access past the check stays inside the scratch)."""
+    row, col, w = grid_graph(20, 20, 1, 10, 0.0, 28)
+    g = mb.HostGraph.from_arrays(row, col, w)
+    n, m = g.n, g.m
+    d = torch.empty(n, dtype=torch.int64, device="cuda")
+    p = torch.empty(n, dtype=torch.int32, device="cuda")
+    bad_row = row.copy()
+    bad_row[-1] = m + 1
+    col_t = torch.from_numpy(np.concatenate([col, [0]]).astype(np.int32)).cuda()
+    w_t = torch.from_numpy(np.concatenate([w[:, 0], [1]]).astype(np.int32)).cuda()
+    row_t = torch.from_numpy(bad_row.astype(np.int32)).cuda()
+    st = mb.SospStats()
+    rc = mb.lib().mosp_sosp_from_scratch_static(n, m, row_t.data_ptr(), col_t.data_ptr(), w_t.data_ptr(), 0, 10,
+                                                10, d.data_ptr(), p.data_ptr(), C.byref(st), None)
+    assert rc == mb.ERR_INVALID
+    bad_col = col.copy()
+    bad_col[7] = n + 5
+    row_t = torch.from_numpy(row.astype(np.int32)).cuda()
+    col_t = torch.from_numpy(bad_col.astype(np.int32)).cuda()
+    rc = mb.lib().mosp_sosp_from_scratch_static(n, m, row_t.data_ptr(), col_t.data_ptr(), w_t.data_ptr(), 0, 10,
+                                                10, d.data_ptr(), p.data_ptr(), C.byref(st), None)
+    assert rc == mb.ERR_INVALID
+    assert b"malformed CSR" in mb.lib().mosp_last_error()
+    # still usable afterwards
+    g2, dg2 = upload(ws, row, col, w)
+    ds, ps, _ = static_tree(g2, dg2, 0, 10, int(w.max()))
+    de, pe = orc.dijkstra(row, col, w, 0, 0)
+    assert np.array_equal(ds, de) and np.array_equal(ps, pe)
