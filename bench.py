@@ -70,7 +70,7 @@ def parse():
     ap.add_argument("--verify", action="store_true", help="check the result against the oracle")
     ap.add_argument("--requests", type=int, default=400, help="serving workload: requests per arrival rate")
     ap.add_argument("--rates", default="50,200,1000", help="serving workload: Poisson arrival rates (1/s)")
-    ap.add_argument("--workload", choices=["road", "powerlaw", "batched", "serving"], default="road",
+    ap.add_argument("--workload", choices=["road", "powerlaw", "batched", "serving", "step1"], default="road",
                     help="road: the road-network update (default); powerlaw: the R-MAT scale-22 update with the "
                          "distance-only fallback; batched: 256 grid-road instances in one launch against "
                          "per-instance launches; serving: the resident-graph request loop")
@@ -895,10 +895,47 @@ def run_reference(args):
         shutil.rmtree(tmp, ignore_errors=True)
 
 
+def run_step1(args):
+    """Step 1 alone (mosp_apply_batch_device: the road workload's batch
+    applied to its graph on the GPU), `steps` timed calls after `warmup`:
+    the driver of the Step 1 profile captures."""
+    import torch
+    import mosp_b200 as mb
+    g, batch, K, _, workload = make_workload(args)
+    ws = mb.Workspace(timeout_ms=60000)
+    row, col, w = g.arrays()
+    ba = batch.arrays()
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    drow, dcol, dw = t(row), t(col), t(w.reshape(-1))
+    ifr, ito, iw = t(ba["ins_from"]), t(ba["ins_to"]), t(ba["ins_w"].reshape(-1))
+    dfr, dto = t(ba["del_from"]), t(ba["del_to"])
+    cap = g.m + batch.n_ins
+    nrow = torch.empty(g.n + 1, dtype=torch.int32, device="cuda")
+    ncol = torch.empty(cap, dtype=torch.int32, device="cuda")
+    nw = torch.empty(cap * K, dtype=torch.int32, device="cuda")
+    mask = torch.empty(max(batch.n_ins, 1), dtype=torch.int32, device="cuda")
+    times = []
+    for i in range(max(args.warmup, 0) + max(args.steps, 1)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ws.apply_batch_device(g.n, K, g.m, drow, dcol, dw, ifr, ito, iw, dfr, dto, nrow, ncol, nw, mask)
+        torch.cuda.synchronize()
+        if i >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    ms = 1000 * float(np.mean(times))
+    print(json.dumps({"metric": "Step 1 (batch application on the GPU) ms", "value": round(ms, 4), "unit": "ms",
+                      "higher_is_better": False, "steps": len(times), "warmup": args.warmup,
+                      "config": {"workload": workload, "n": g.n, "m": g.m,
+                                 "changes": int(batch.n_ins + batch.n_del)}}), flush=True)
+    ws.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "step1":
+        run_step1(args)
     elif args.workload == "batched":
         run_batched(args)
     elif args.workload == "serving":
