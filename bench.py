@@ -64,8 +64,9 @@ def parse():
     ap.add_argument("--changes", type=int, default=50000)
     ap.add_argument("--delta", type=int, default=0, help="fixed near-far width (0: default heuristic)")
     ap.add_argument("--e2e-steps", type=int, default=5)
-    ap.add_argument("--loop", choices=["async", "bulk"], default="async",
-                    help="near-far loop of the persistent launches (results are the same)")
+    ap.add_argument("--loop", choices=["auto", "async", "bulk"], default="auto",
+                    help="near-far loop of the persistent launches: auto = the autotuner's choice "
+                         "(results are the same)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--verify", action="store_true", help="check the result against the oracle")
     ap.add_argument("--requests", type=int, default=400, help="serving workload: requests per arrival rate")
@@ -211,7 +212,7 @@ def run_ours(args):
     n, src = g.n, 0
     ws = mb.Workspace(timeout_ms=60000)
     ws.enable_timing(True)
-    ws.set_async(args.loop == "async")
+    ws.set_async(args.loop != "bulk")
     row, col, w = g.arrays()
     # initial canonical trees of the original graph (GPU engine, from scratch)
     dg0 = mb.DeviceGraph.upload(ws, g)
@@ -276,6 +277,9 @@ def run_ours(args):
     else:
         tuned = deltas
         rounds = (0, 2)
+    if args.loop != "auto":
+        ws.set_async(args.loop == "async")
+    grid_ctas, hub_edges, async_on = ws.tuning()
     for _ in range(max(args.warmup, 0)):
         step(False, tuned)
     torch.cuda.synchronize()
@@ -340,7 +344,8 @@ def run_ours(args):
         # the same widths and local rounds as the device-resident steps, set
         # through the public API
         host_ws = mb.Workspace(timeout_ms=60000)
-        host_ws.set_async(args.loop == "async")
+        host_ws.set_async(async_on)
+        host_ws.set_grid(grid_ctas, hub_edges)
         host_ws.set_combined_delta(comb_delta)
         host_ws.set_local_rounds(*rounds)
         pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
@@ -386,7 +391,9 @@ def run_ours(args):
                            "local_rounds": {"update": rounds[0], "combined": rounds[1]},
                            "delta_default": deltas,
                            "widths": "autotuned (mosp_autotune_update)" if args.delta <= 0 else "fixed by --delta",
-                           "near_far_loop": args.loop, "grid_ctas": ws.grid()},
+                           "near_far_loop": ("asynchronous" if async_on else "bulk-synchronous")
+                           + (" (autotuned)" if args.loop == "auto" else " (forced)"),
+                           "grid_ctas": grid_ctas, "hub_row_edges": hub_edges},
                 "gpu_compute_ms": round(ms_per_step, 4),
                 "default_widths_ms_per_step": round(float(np.mean(default_ms)), 4),
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,

@@ -195,6 +195,20 @@ int mosp_workspace_set_timeout_ms(mosp_workspace *ws, long long ms);
  * fit). Results do not depend on it. */
 int mosp_workspace_set_ctas_per_sm(mosp_workspace *ws, int ctas_per_sm);
 
+/* Grid and hub threshold of the persistent engine launches. ctas = 0 uses
+ * one 1,024-thread CTA per SM on every SM (the occupancy-sized grid of the
+ * reference, src/sospUpdateGpu.cu:553-595); a smaller count launches fewer
+ * CTAs (cheaper grid barriers, fewer warps). hub_edges (0 = 2,048, else at
+ * least 64): rows with more edges are expanded and reduced by a whole CTA,
+ * and a graph with such rows runs the bulk near-far loop. Results do not
+ * depend on either; mosp_autotune_update picks both. No counterpart in the
+ * reference. */
+int mosp_workspace_set_grid(mosp_workspace *ws, int ctas, int hub_edges);
+
+/* The workspace's current engine settings: grid CTAs, hub threshold and
+ * near-far loop (1 asynchronous, 0 bulk), e.g. after mosp_autotune_update. */
+int mosp_workspace_tuning(mosp_workspace *ws, int *ctas, int *hub_edges, int *async_on);
+
 /* Grid size (CTAs) the persistent kernels use on this device. */
 int mosp_workspace_grid(mosp_workspace *ws, int *ctas);
 
@@ -410,9 +424,14 @@ int mosp_update_device(mosp_workspace *ws, int n, int m, int K,
  * mosp_workspace_set_local_rounds; may be NULL) and their summed launch
  * time (*h_best_ms, may be NULL). The trees d_dist /
  * d_parent are restored to their input values before returning; results of
- * later updates do not depend on the widths chosen. It allocates a copy of
- * the trees for the duration of the call. No counterpart in the reference
- * (its width is the fixed heuristic of defaultDelta). */
+ * later updates do not depend on the widths chosen. With the best widths
+ * it then times the near-far loop (asynchronous or bulk), two smaller grids
+ * (3/4 and 1/2 of the CTAs) and, when the graph has hub rows, hub
+ * thresholds of 16,384 and 2^20 edges, and leaves the fastest of those set
+ * on the workspace (mosp_workspace_tuning reads them). It allocates a copy
+ * of the trees for the duration of the call. No counterpart in the
+ * reference (its width is the fixed heuristic of defaultDelta and its grid
+ * the occupancy-sized one). */
 int mosp_autotune_update(mosp_workspace *ws, int n, int m, int K,
                          const int *d_out_row, const int *d_out_col,
                          const int *d_out_w, const int *d_in_row,

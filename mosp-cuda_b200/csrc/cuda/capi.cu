@@ -80,6 +80,12 @@ struct mosp_workspace {
   // hub rows, so the next one goes straight to the bulk loop with its full
   // stage
   bool heavySeen[2] = {false, false};
+  // grid of the persistent engine launches (0: one CTA per SM, all SMs) and
+  // the hub-row threshold (0: the engine's default); autotuned, results do
+  // not depend on them
+  int gridCtas = 0;
+  int heavyDeg = 0;
+  int graphCtas = 0;  // grid of the captured CUDA graph
   // control blocks
   EngineControl *ctl = nullptr;
   EngineControl *hostCtl = nullptr;  // pinned
@@ -177,6 +183,13 @@ void releaseLists(mosp_workspace *ws) {
   ws->kCap = 0;
   releaseNear(ws);
   releaseAsync(ws);
+}
+
+/// CTAs of an engine launch: the occupancy-sized grid, or fewer when the
+/// workspace asks for it.
+int engineCtas(const mosp_workspace *ws) {
+  const int full = ws->shape.engineCtas;
+  return ws->gridCtas > 0 && ws->gridCtas < full ? ws->gridCtas : full;
 }
 
 int ensureShape(mosp_workspace *ws) {
@@ -367,6 +380,7 @@ void fillLists(EngineParams &p, mosp_workspace *ws, int block) {
   p.sources = ws->nSources > 1 ? ws->sources : nullptr;
   p.nSources = ws->nSources > 1 ? ws->nSources : 0;
   p.flags = engineFlags();
+  p.heavyDeg = ws->heavyDeg;
   // asynchronous loop unless it is off or the graph last seen here had hub
   // rows; its launches need a smaller stage (the pull pass stays staged up
   // to K tiles), which leaves more of the SM's memory to L1
@@ -435,11 +449,11 @@ int queueEngine(mosp_workspace *ws, const EngineParams &p, int block, cudaStream
     // distance-only objectives: the parent recovery follows as its own kernel
     EngineParams q = p;
     q.flags |= kFlagHostRecovery;
-    MOSP_CUDA(launchEngine(q, ws->shape.engineCtas, s));
+    MOSP_CUDA(launchEngine(q, engineCtas(ws), s));
     MOSP_CUDA(launchRecovery(q, s));
     return MOSP_OK;
   }
-  MOSP_CUDA(launchEngine(p, ws->shape.engineCtas, s));
+  MOSP_CUDA(launchEngine(p, engineCtas(ws), s));
   return MOSP_OK;
 }
 
@@ -459,7 +473,7 @@ int readControl(mosp_workspace *ws, int first, int count, cudaStream_t s) {
 /// replayed on `s` otherwise. The caller waits on `s`.
 int launchUpdateGraph(mosp_workspace *ws, const EngineParams &pu, const EngineParams &pc,
                       cudaStream_t s) {
-  const bool same = ws->graphExec != nullptr &&
+  const bool same = ws->graphExec != nullptr && ws->graphCtas == engineCtas(ws) &&
                     std::memcmp(&ws->graphPu, &pu, sizeof(EngineParams)) == 0 &&
                     std::memcmp(&ws->graphPc, &pc, sizeof(EngineParams)) == 0;
   if (!same) {
@@ -476,13 +490,13 @@ int launchUpdateGraph(mosp_workspace *ws, const EngineParams &pu, const EnginePa
     if (needsHostRecovery(pu)) {
       EngineParams q = pu;
       q.flags |= kFlagHostRecovery;
-      if (err == cudaSuccess) err = launchEngineEx(q, ws->shape.engineCtas, c);
+      if (err == cudaSuccess) err = launchEngineEx(q, engineCtas(ws), c);
       if (err == cudaSuccess) err = launchRecovery(q, c);
     } else if (err == cudaSuccess) {
-      err = launchEngineEx(pu, ws->shape.engineCtas, c);
+      err = launchEngineEx(pu, engineCtas(ws), c);
     }
     if (err == cudaSuccess) err = cudaMemsetAsync(ws->ctl + 1, 0, sizeof(EngineControl), c);
-    if (err == cudaSuccess) err = launchEngineEx(pc, ws->shape.engineCtas, c);
+    if (err == cudaSuccess) err = launchEngineEx(pc, engineCtas(ws), c);
     if (err == cudaSuccess) {
       err = cudaMemcpyAsync(ws->hostCtl, ws->ctl, 2 * sizeof(EngineControl),
                             cudaMemcpyDeviceToHost, c);
@@ -499,6 +513,7 @@ int launchUpdateGraph(mosp_workspace *ws, const EngineParams &pu, const EnginePa
     }
     ws->graphPu = pu;
     ws->graphPc = pc;
+    ws->graphCtas = engineCtas(ws);
   }
   MOSP_CUDA(cudaGraphLaunch(ws->graphExec, s));
   ++ws->graphReplays;
@@ -827,6 +842,24 @@ int mosp_workspace_set_async(mosp_workspace *ws, int on, long long queue_slots) 
   return MOSP_OK;
 }
 
+int mosp_workspace_set_grid(mosp_workspace *ws, int ctas, int hub_edges) {
+  if (ws == nullptr || ctas < 0 || hub_edges < 0 || (hub_edges > 0 && hub_edges < 64)) {
+    return fail(MOSP_ERR_INVALID, "invalid grid settings");
+  }
+  ws->gridCtas = ctas;
+  ws->heavyDeg = hub_edges;
+  return MOSP_OK;
+}
+
+int mosp_workspace_tuning(mosp_workspace *ws, int *ctas, int *hub_edges, int *async_on) {
+  int st = checkWorkspace(ws);
+  if (st != MOSP_OK) return st;
+  if (ctas) *ctas = engineCtas(ws);
+  if (hub_edges) *hub_edges = ws->heavyDeg > 0 ? ws->heavyDeg : 2048;
+  if (async_on) *async_on = ws->asyncMode;
+  return MOSP_OK;
+}
+
 int mosp_workspace_use_graphs(mosp_workspace *ws, int on) {
   int st = checkWorkspace(ws);
   if (st != MOSP_OK) return st;
@@ -915,7 +948,7 @@ int mosp_workspace_loop_profile(mosp_workspace *ws, int which, unsigned long lon
 int mosp_workspace_grid(mosp_workspace *ws, int *ctas) {
   int st = checkWorkspace(ws);
   if (st != MOSP_OK) return st;
-  if (ctas) *ctas = ws->shape.engineCtas;
+  if (ctas) *ctas = engineCtas(ws);
   return MOSP_OK;
 }
 
@@ -1341,6 +1374,76 @@ int mosp_autotune_update(mosp_workspace *ws, int n, int m, int K, const int *d_o
     h_best_delta[k] = std::max(1LL, static_cast<long long>(h_delta[k] * bestUc.factor));
   }
   *h_best_comb_delta = bestComb;
+
+  // With those widths: the near-far loop (asynchronous or bulk), the grid
+  // (all SMs, or fewer CTAs: cheaper grid barriers) and, for graphs with
+  // hub rows, the hub threshold (a higher one lets the asynchronous loop
+  // run). Timed on the whole update; the best stays set on the workspace.
+  {
+    for (int k = 0; k < K; ++k) deltas[k] = h_best_delta[k];
+    ws->roundsUpdate = bestUc.rounds;
+    ws->roundsScratch = bestCr;
+    ws->combDelta = bestComb;
+    auto timeIt = [&](float &total) -> int {
+      total = 1e30f;
+      for (int rep = 0; rep < 2; ++rep) {
+        MOSP_CUDA(cudaMemcpyAsync(d_dist, saveDist, kn * sizeof(long long), cudaMemcpyDeviceToDevice, s));
+        MOSP_CUDA(cudaMemcpyAsync(d_parent, saveParent, kn * sizeof(int), cudaMemcpyDeviceToDevice, s));
+        const int rc = mosp_update_device(ws, n, m, K, d_out_row, d_out_col, d_out_w, d_in_row, d_in_col,
+                                          d_in_w, d_changed_from, d_changed_to, h_changed_offset,
+                                          d_insert_heads, n_heads, source, deltas.data(), h_max_weight,
+                                          h_pref, d_dist, d_parent, d_comb_dist, d_comb_parent, nullptr,
+                                          nullptr, stream);
+        if (rc != MOSP_OK) return rc;
+        total = std::min(total, ws->lastUpdateMs + ws->lastCombinedMs);
+      }
+      return MOSP_OK;
+    };
+    struct Shape {
+      int async, grid, hub;
+    };
+    const int full = ws->shape.engineCtas;
+    const bool hubs = ws->heavySeen[0] || ws->heavySeen[1];
+    Shape best{ws->asyncMode, ws->gridCtas, ws->heavyDeg};
+    float bestMs = 1e30f;
+    auto trial = [&](Shape sh) -> int {
+      ws->asyncMode = sh.async;
+      ws->gridCtas = sh.grid;
+      ws->heavyDeg = sh.hub;
+      ws->heavySeen[0] = ws->heavySeen[1] = false;
+      if (sh.async != 0) {
+        int rc = reserveAsync(ws, n, K);
+        if (rc != MOSP_OK) return rc;
+      }
+      float ms = 0;
+      const int rc = timeIt(ms);
+      if (rc != MOSP_OK) return rc;
+      if (ms < bestMs) {
+        bestMs = ms;
+        best = sh;
+      }
+      return MOSP_OK;
+    };
+    const Shape start = best;
+    if ((st = trial(start)) != MOSP_OK) return st;
+    if ((st = trial(Shape{1 - start.async, start.grid, start.hub})) != MOSP_OK) return st;
+    for (int grid : {full * 3 / 4, full / 2}) {
+      if (grid >= 1 && (st = trial(Shape{best.async, grid, best.hub})) != MOSP_OK) return st;
+    }
+    if (hubs) {
+      for (int hub : {16384, 1 << 20}) {
+        if ((st = trial(Shape{1, best.grid, hub})) != MOSP_OK) return st;
+      }
+    }
+    ws->asyncMode = best.async;
+    ws->gridCtas = best.grid;
+    ws->heavyDeg = best.hub;
+    ws->heavySeen[0] = ws->heavySeen[1] = false;
+    if (bestMs < bestU + bestC) {
+      bestU = bestMs;
+      bestC = 0;
+    }
+  }
   if (h_best_rounds) {
     h_best_rounds[0] = bestUc.rounds;
     h_best_rounds[1] = bestCr;

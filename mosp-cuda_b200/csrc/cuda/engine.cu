@@ -253,8 +253,14 @@ constexpr int kStage = kStageEntriesMax;
 // otherwise keep one warp busy for the whole iteration. A launch turns
 // this on only when its graph has such rows (EngineControl::heavy, set in
 // the first phase), so graphs without them take no extra CTA barriers.
-constexpr int kHeavyDeg = 2048;
+constexpr int kHeavyDegDefault = 2048;  // EngineParams::heavyDeg when 0
 constexpr int kHeavyCap = 64;
+
+/// Rows above this many edges go to a whole CTA (and keep a launch in the
+/// bulk loop); a launch parameter, so the autotuner can move it.
+__device__ __forceinline__ int heavyDegOf(const EngineParams &P) {
+  return P.heavyDeg > 0 ? P.heavyDeg : kHeavyDegDefault;
+}
 
 struct StageHeader {
   int cap;                     // entries per list partition (kStage / (2K))
@@ -619,7 +625,7 @@ __device__ __forceinline__ void expandWarp(const EngineParams &P, const LoopShar
   if (__ballot_sync(kFull, deg > 0) == 0) return;
   // heavy rows go to the CTA's queue (expanded by the whole CTA after this
   // round of items) when the launch has any
-  if (heavyOn && deg > kHeavyDeg) {
+  if (heavyOn && deg > heavyDegOf(P)) {
     const int slot = atomicAdd(&H.heavyCount, 1);
     if (slot < kHeavyCap) {
       H.heavyK[slot] = k;
@@ -1596,9 +1602,10 @@ __global__ void __launch_bounds__(kThreads, 1) sospEngine(const __grid_constant_
   }
   if constexpr (Mode == kModeUpdate) {
     // ---- Heavy rows: does the graph have rows for whole-CTA handling? -----
+    const int heavyDeg = heavyDegOf(P);
     for (long long v = tid; v < n; v += T) {
-      if (__ldg(outRow + v + 1) - __ldg(outRow + v) > kHeavyDeg ||
-          __ldg(P.inRow + v + 1) - __ldg(P.inRow + v) > kHeavyDeg) {
+      if (__ldg(outRow + v + 1) - __ldg(outRow + v) > heavyDeg ||
+          __ldg(P.inRow + v + 1) - __ldg(P.inRow + v) > heavyDeg) {
         c->heavy = 1;
       }
     }
@@ -1819,7 +1826,7 @@ __global__ void __launch_bounds__(kThreads, 1) sospEngine(const __grid_constant_
           end = __ldg(P.inRow + v + 1);
         }
         // heavy in-rows are reduced by the whole CTA after the tile
-        if (heavyOn && end - beg > kHeavyDeg) {
+        if (heavyOn && end - beg > heavyDegOf(P)) {
           const int slot = atomicAdd(&H.heavyCount, 1);
           if (slot < kHeavyCap) {
             H.heavyK[slot] = k;
@@ -2046,7 +2053,7 @@ __device__ void scratchOrCombined(const EngineParams &P, Sync &epoch, int genBas
 
   // ---- SSSP from scratch: only the source (the roots) is finite ------------
   for (long long v = tid; v < n; v += T) {
-    if (ldGraph<Mode>(outRow + v + 1) - ldGraph<Mode>(outRow + v) > kHeavyDeg) c->heavy = 1;
+    if (ldGraph<Mode>(outRow + v + 1) - ldGraph<Mode>(outRow + v) > heavyDegOf(P)) c->heavy = 1;
   }
   for (int k = 0; k < K; ++k) {
     const Pk pk = pkOf(P.obj[k]);

@@ -163,6 +163,7 @@ struct EngineParams {
   unsigned aqShardCap;
   int aqShards;
   int stageEntries;            // entries of the per-CTA append stage (dynamic shared memory)
+  int heavyDeg;                // rows above this many edges: whole-CTA handling (0: 2,048)
   EngineControl *ctl;
   // combined graph (Steps 2-3)
   const int *combParents;      // K trees, objective-major

@@ -84,6 +84,8 @@ _SIGS = {
     "mosp_workspace_set_local_rounds": (_i, [_p, _i, _i]),
     "mosp_workspace_set_narrow": (_i, [_p, _i, _i]),
     "mosp_workspace_set_async": (_i, [_p, _i, _ll]),
+    "mosp_workspace_set_grid": (_i, [_p, _i, _i]),
+    "mosp_workspace_tuning": (_i, [_p, _ip, _ip, _ip]),
     "mosp_workspace_graph_launches": (_i, [_p, _ip]),
     "mosp_autotune_update": (_i, [_p, _i, _i, _i, _p, _p, _p, _p, _p, _p, _p, _p, _ip, _p, _i, _i,
                                   _llp, _llp, _ip, _p, _p, _p, _p, _llp, _llp, _ip, C.POINTER(C.c_float), _p]),
@@ -505,6 +507,16 @@ class Workspace:
 
     def set_narrow(self, max_items, rounds):
         check(lib().mosp_workspace_set_narrow(self._h, int(max_items), int(rounds)))
+
+    def set_grid(self, ctas=0, hub_edges=0):
+        """Grid CTAs of the engine launches (0: all SMs) and hub-row threshold (0: default)."""
+        check(lib().mosp_workspace_set_grid(self._h, int(ctas), int(hub_edges)))
+
+    def tuning(self):
+        """(grid CTAs, hub threshold, asynchronous loop on) of the workspace."""
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        check(lib().mosp_workspace_tuning(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, bool(c.value)
 
     def set_async(self, on=True, queue_slots=0):
         """Asynchronous near-far loop (default) or the bulk-synchronous one;

@@ -123,3 +123,50 @@ def test_graph_replay(ws, case):
         assert ws.graph_launches() - start == 4
     finally:
         ws.use_graphs(False)
+
+
+@pytest.mark.parametrize("loop", [True, False])
+@pytest.mark.parametrize("ctas,hub", [(0, 0), (37, 0), (74, 64), (1, 0), (0, 1 << 20)])
+def test_grid_and_hub_threshold_keep_results(case, loop, ctas, hub):
+    """Every engine knob the autotuner searches (near-far loop, grid CTAs,
+    hub-row threshold, incl. a grid of one CTA and a threshold so low that
+    every longer row goes to the CTA-wide path) leaves the results equal to
+    the oracle."""
+    K, g0, g, b, upd, ba, exp, d0, p0 = case
+    w = mb.Workspace(timeout_ms=20000)
+    try:
+        w.set_async(loop)
+        w.set_grid(ctas, hub)
+        dg, cf, ct, off, heads, maxw, deltas = args_for(w, case)
+        dist, par = dev(d0), dev(p0)
+        cd = torch.empty(upd.n, dtype=torch.int64, device="cuda")
+        cp = torch.empty(upd.n, dtype=torch.int32, device="cuda")
+        run(w, case, dg, cf, ct, off, heads, maxw, deltas, dist, par, cd, cp)
+        check(exp, dist, par, cd, cp)
+        got = w.tuning()
+        assert got[2] == loop and (ctas == 0 or got[0] == ctas)
+    finally:
+        w.close()
+
+
+def test_autotuner_leaves_engine_settings_consistent(case):
+    """After the autotuner the workspace holds its choice of loop, grid and
+    hub threshold, and an update with them reproduces the oracle."""
+    K, g0, g, b, upd, ba, exp, d0, p0 = case
+    w = mb.Workspace(timeout_ms=20000)
+    try:
+        dg, cf, ct, off, heads, maxw, deltas = args_for(w, case)
+        dist, par = dev(d0), dev(p0)
+        cd = torch.empty(upd.n, dtype=torch.int64, device="cuda")
+        cp = torch.empty(upd.n, dtype=torch.int32, device="cuda")
+        best, comb, _, rounds = w.autotune_update(upd.n, upd.m, K, dg.out_row, dg.out_col, dg.out_w, dg.in_row,
+                                                  dg.in_col, dg.in_w, cf, ct, off, heads, len(ba["ins_to"]), 0,
+                                                  deltas, maxw, None, dist, par, cd, cp)
+        ctas, hub, loop = w.tuning()
+        assert ctas >= 1 and hub >= 64
+        w.set_combined_delta(comb)
+        w.set_local_rounds(*rounds)
+        run(w, case, dg, cf, ct, off, heads, maxw, best, dist, par, cd, cp)
+        check(exp, dist, par, cd, cp)
+    finally:
+        w.close()
