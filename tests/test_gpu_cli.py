@@ -156,3 +156,31 @@ def test_byte_identical_to_reference_binary(prepared, batch):
     assert len(files) == 3 * 2 + 3
     for rel in files:
         assert filecmp.cmp(a / rel, b / rel, shallow=False), str(rel)
+
+
+PREP_REF = os.path.join(ROOT, "oracle", "_ref", "mospPrep_ref")
+
+
+@pytest.mark.parametrize("source", [0, 17])
+def test_mosp_prep_gpu_trees_equal_host_and_reference(prepared, tmp_path, source):
+    """`mospPrep init --gpu` and `expected --gpu` (the canonical GPU SSSP for
+    every objective, one workspace reused across objectives) write the same
+    files byte for byte as the host Dijkstra path and, where it was built,
+    the reference's own mospPrep (src/mospPrep.cu:350-375)."""
+    g = prepared / "g"
+    csr = g / "csr/graphCsr"
+    outs = {}
+    for name, tool, extra in [("host", PREP, []), ("gpu", PREP, ["--gpu"]), ("ref", PREP_REF, [])]:
+        if name == "ref" and not os.path.exists(PREP_REF):
+            continue
+        d = tmp_path / name
+        run([tool, "init", csr, d / "init", "--source", source] + extra, prepared)
+        run([tool, "expected", csr, g / "unsafe", d / "expected", "--source", source] + extra, prepared)
+        outs[name] = d
+    files = [f"{stage}/obj{k}/{kind}" for k in range(3)
+             for stage, kind in (("init", "distancesOriginal.txt"), ("init", "SSSPTreeOriginal.txt"),
+                                 ("expected", "distancesUpdated.txt"), ("expected", "SSSPTreeUpdated.txt"))]
+    for f in files:
+        for name in outs:
+            if name != "host":
+                assert filecmp.cmp(outs["host"] / f, outs[name] / f, shallow=False), (name, f)
