@@ -9,6 +9,8 @@
 #include "changeGenerator.cuh"
 
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <filesystem>
@@ -23,6 +25,7 @@
 #include <vector>
 
 #include "csrGraph.cuh"
+#include "deletionFilter.h"
 #include "dijkstra.cuh"
 #include "mospGenerators.h"
 
@@ -55,6 +58,7 @@ std::vector<int> ball(const CsrGraph &g, const CsrGraph &rev, int centre, int ho
   return order;
 }
 
+/// Vertices reachable from source (host BFS over the out-edges).
 std::vector<char> reachable(const CsrGraph &g, int source) {
   std::vector<char> seen(g.numberOfNodes, 0);
   std::vector<int> queue{source};
@@ -72,42 +76,30 @@ std::vector<char> reachable(const CsrGraph &g, int source) {
   return seen;
 }
 
+std::atomic<bool> g_filterOnGpu{false};
+double g_lastFilterMs = 0;
+
 }  // namespace
 
-/// Drop deletions until no vertex reachable from source before the batch
-/// becomes unreachable after it; returns the number of rounds.
 int filterUnsafeDeletions(const CsrGraph &g, int source, ChangeBatch &batch) {
-  const std::vector<char> before = reachable(g, source);
-  int rounds = 0;
-  while (batch.numberOfDeletes() > 0) {
-    ++rounds;
-    ChangeBatch trial = batch;
-    CsrGraph after;
-    applyChangeBatch(g, trial, after);
-    const std::vector<char> now = reachable(after, source);
-    std::vector<char> lost(g.numberOfNodes, 0);
-    bool any = false;
-    for (int v = 0; v < g.numberOfNodes; ++v) {
-      if (before[v] && !now[v]) {
-        lost[v] = 1;
-        any = true;
-      }
-    }
-    if (!any) break;
-    std::vector<int> from, to;
-    for (int i = 0; i < batch.numberOfDeletes(); ++i) {
-      const int u = batch.deleteFrom[i], v = batch.deleteTo[i];
-      if (!lost[u] && !lost[v]) {
-        from.push_back(u);
-        to.push_back(v);
-      }
-    }
-    if (static_cast<int>(from.size()) == batch.numberOfDeletes()) break;
-    batch.deleteFrom.swap(from);
-    batch.deleteTo.swap(to);
+  const auto t0 = std::chrono::steady_clock::now();
+  int rounds = -1;
+  if (g_filterOnGpu.load()) rounds = filterUnsafeDeletionsGpu(g, source, batch);
+  if (rounds < 0) {
+    rounds = filterDeletionRounds(reachable(g, source), batch, [&](const ChangeBatch &b) {
+      ChangeBatch applied = b;
+      CsrGraph updated;
+      applyChangeBatch(g, applied, updated);
+      return reachable(updated, source);
+    });
   }
+  g_lastFilterMs = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   return rounds;
 }
+
+void useGpuDeletionFilter(bool on) { g_filterOnGpu.store(on); }
+
+double lastDeletionFilterMs() { return g_lastFilterMs; }
 
 bool parseChangeMode(const std::string &name, ChangeMode &mode) {
   if (name == "uniform") {

@@ -6,7 +6,7 @@
 //   mospPrep mtx2csr <in.mtx> <outPrefix> <K> <wmin> <wmax> <seed>
 //   mospPrep widen <inPrefix> <outPrefix> <K> <wmin> <wmax> <seed>
 //   mospPrep cache <csrPrefix> <binaryPath>
-//   mospPrep changes <csrPrefix> <outDir> [--changes N] [--ins PCT]
+//   mospPrep changes <csrPrefix> <outDir> [--changes N] [--ins PCT] [--gpu]
 //            [--mode uniform|targeted|reweight|increase] [--local HOPS]
 //            [--safe] [--seed S] [--source s] [--wmin a] [--wmax b]
 //   mospPrep init <csrPrefix> <outDir> [--source s] [--gpu]
@@ -214,6 +214,10 @@ bool changeOptions(int argc, char **argv, int first, ChangeGeneratorOptions &o) 
       o.safeDeletions = true;
       continue;
     }
+    if (a == "--gpu") {  // the --safe filter's reachability on the GPU
+      useGpuDeletionFilter(true);
+      continue;
+    }
     if (i + 1 >= argc) {
       std::cerr << "missing value for " << a << "\n";
       return false;
@@ -357,6 +361,7 @@ int main(int argc, char **argv) {
              ? 0
              : 1;
     std::cout << "changes: " << report << "\n";
+    if (o.safeDeletions) std::cout << "safe filter: " << lastDeletionFilterMs() << " ms\n";
   } else if (cmd == "init" && argc >= 4) {
     CsrGraph g;
     if (!readCsrGraph(argv[2], g)) {

@@ -38,4 +38,19 @@ bool generateNearBatch(const CsrGraph &graph, int gridWidth, int nIns, int nDel,
 /// number of filter rounds.
 int filterUnsafeDeletions(const CsrGraph &graph, int source, ChangeBatch &batch);
 
+/// The same filter with reachability computed on the current GPU: each
+/// round applies the batch with Step 1 (mosp_apply_batch_device) and runs a
+/// unit-weight SSSP from the source on the engine. Same rounds and the
+/// same kept deletions as the host filter. Returns the rounds, or -1 if a
+/// GPU step failed (the batch is then unchanged).
+int filterUnsafeDeletionsGpu(const CsrGraph &graph, int source, ChangeBatch &batch);
+
+/// Route filterUnsafeDeletions (and so `--safe` batches of
+/// generateChangeBatch) to the GPU path; it falls back to the host when a
+/// GPU step fails.
+void useGpuDeletionFilter(bool on);
+
+/// Wall time (ms) of the last filterUnsafeDeletions call.
+double lastDeletionFilterMs();
+
 #endif // MOSP_B200_GENERATORS_H

@@ -52,10 +52,6 @@ def test_async_equals_bulk_and_oracle(gpu, spec):
     for key in KEYS:
         assert np.array_equal(outs[0][key], outs[1][key]), key
     assert_matches_oracle(outs[0], g, b)
-    # the asynchronous loop needs a few phases where the bulk loop iterates
-    phases = sum(s.iterations for s in outs[0]["stats"])
-    iterations = sum(s.iterations for s in outs[1]["stats"])
-    assert phases <= iterations
 
 
 def test_async_small_queue_overflows_to_far(gpu):

@@ -184,3 +184,30 @@ def test_mosp_prep_gpu_trees_equal_host_and_reference(prepared, tmp_path, source
         for name in outs:
             if name != "host":
                 assert filecmp.cmp(outs["host"] / f, outs[name] / f, shallow=False), (name, f)
+
+
+@pytest.mark.parametrize("width,changes,extra", [(120, 4000, []), (200, 20000, ["--mode", "targeted"]),
+                                                 (90, 3000, ["--local", "6"])])
+def test_safe_filter_on_gpu_equals_host_and_reference(tmp_path, width, changes, extra):
+    """`mospPrep changes --safe --gpu` (the connectivity filter's rounds with
+    reachability from Step 1 and a unit-weight SSSP on the GPU) writes the
+    same insert.txt / delete.txt as the host filter and as the reference's
+    own mospPrep (src/changeGenerator.cu:78-114)."""
+    csr = tmp_path / "csr/graphCsr"
+    run([PREP, "grid", csr, width, width, "0.7", "0.01", 2, 1, 50, 12345], tmp_path)
+    outs = {}
+    for name, tool, flag in [("host", PREP, []), ("gpu", PREP, ["--gpu"]), ("ref", PREP_REF, [])]:
+        if name == "ref" and not os.path.exists(PREP_REF):
+            continue
+        d = tmp_path / name
+        r = run([tool, "changes", csr, d, "--changes", changes, "--seed", 777, "--safe"] + extra + flag, tmp_path)
+        if name != "ref":
+            assert "safe filter:" in r.stdout
+        outs[name] = d
+    for f in ("insert.txt", "delete.txt"):
+        for name in outs:
+            assert filecmp.cmp(outs["host"] / f, outs[name] / f, shallow=False), (name, f)
+    # the filter dropped something, so the rounds ran
+    full = tmp_path / "unsafe"
+    run([PREP, "changes", csr, full, "--changes", changes, "--seed", 777] + extra, tmp_path)
+    assert os.path.getsize(full / "delete.txt") >= os.path.getsize(outs["gpu"] / "delete.txt")
