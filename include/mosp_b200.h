@@ -505,9 +505,11 @@ int mosp_debug_barrier_cost(mosp_workspace *ws, int rounds, int reads,
  * engine update with the union of their change lists, which gives the
  * same trees as applying them one by one); a pass starts only when the memory it may
  * allocate fits in the free device memory minus `reserve_bytes` (unless no
- * pass is running). The persistent launches of different workers run one
- * at a time (each fills the GPU); the workers' copies and host work overlap
- * with them. No counterpart in the reference, which runs one update per
+ * pass is running). With W > 1 workers each worker's persistent launches
+ * use 1/W of the SMs, so the passes of different workers run on the device
+ * at the same time (mosp_server_set_overlap turns this off: one pass's
+ * launches at a time, each on the whole GPU); copies and host work overlap
+ * in both modes. No counterpart in the reference, which runs one update per
  * invocation. */
 typedef struct mosp_server mosp_server;
 
@@ -530,7 +532,8 @@ typedef struct mosp_server_stats {
   long long deferred;  /* times a graph's pass waited for device memory */
   long long applies;   /* Step 1 runs (merged batches; > passes on conflicts) */
   int max_coalesced;
-  int reserved;
+  int overlapped;      /* passes whose engine launches ran while another
+                          pass's did (on disjoint SMs) */
   double busy_us;      /* summed pass durations over the workers */
   double apply_us;     /* of which: uploads, Step 1, change lists */
   double engine_us;    /* graph build + update + combined (incl. lock wait) */
@@ -572,6 +575,11 @@ int mosp_server_read_graph(mosp_server *server, int graph_id,
                            int *h_comb_parent);
 
 int mosp_server_get_stats(mosp_server *server, mosp_server_stats *out);
+
+/* on = 1 (default): passes of different workers share the device (1/W of
+ * the SMs each); 0: one pass's launches at a time on the whole GPU. Set it
+ * before submitting work. */
+int mosp_server_set_overlap(mosp_server *server, int on);
 
 #ifdef __cplusplus
 }

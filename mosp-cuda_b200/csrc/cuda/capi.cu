@@ -185,12 +185,14 @@ void releaseLists(mosp_workspace *ws) {
   releaseAsync(ws);
 }
 
-/// CTAs of an engine launch: the occupancy-sized grid, or fewer when the
-/// workspace asks for it.
-int engineCtas(const mosp_workspace *ws) {
-  const int full = ws->shape.engineCtas;
+/// CTAs of a persistent launch whose occupancy-sized grid is `full`: that
+/// grid, or fewer when the workspace asks for it (also what keeps several
+/// workspaces' cooperative grids on disjoint SMs).
+int limitCtas(const mosp_workspace *ws, int full) {
   return ws->gridCtas > 0 && ws->gridCtas < full ? ws->gridCtas : full;
 }
+
+int engineCtas(const mosp_workspace *ws) { return limitCtas(ws, ws->shape.engineCtas); }
 
 int ensureShape(mosp_workspace *ws) {
   if (ws->shapeValid) return MOSP_OK;
@@ -983,7 +985,7 @@ int mosp_build_device_graph(mosp_workspace *ws, int n, int m, int K, const int *
   b.blockSums = ws->blockSums;
   b.ctl = ws->ctl + 2;
   MOSP_CUDA(cudaMemsetAsync(ws->ctl + 2, 0, sizeof(EngineControl), s));
-  MOSP_CUDA(launchBuild(b, ws->shape.buildCtas, s));
+  MOSP_CUDA(launchBuild(b, limitCtas(ws, ws->shape.buildCtas), s));
   if ((st = readControl(ws, 2, 1, s)) != MOSP_OK) return st;
   const EngineControl &c = ws->hostCtl[2];
   if (c.status != 0) return fail(MOSP_ERR_TIMEOUT, "Error: device graph build timed out.");
@@ -1498,7 +1500,7 @@ int mosp_path_costs(mosp_workspace *ws, int n, int m, int KG, const int *d_out_r
   c.costs = d_costs;
   c.ctl = ws->ctl + 3;
   MOSP_CUDA(cudaMemsetAsync(ws->ctl + 3, 0, sizeof(EngineControl), s));
-  MOSP_CUDA(launchCosts(c, ws->shape.costCtas, s));
+  MOSP_CUDA(launchCosts(c, limitCtas(ws, ws->shape.costCtas), s));
   if ((st = readControl(ws, 3, 1, s)) != MOSP_OK) return st;
   const EngineControl &h = ws->hostCtl[3];
   if (h.status != 0) return fail(MOSP_ERR_TIMEOUT, "Error: path-cost kernel timed out.");

@@ -20,13 +20,14 @@
 //   * admission by free device memory: a pass starts only when the memory it
 //     may allocate (CSR growth, Step 1 scratch, staging) fits in the free
 //     device memory minus a reserve, unless nothing else is running;
-//   * overlap: the persistent cooperative launches (graph build, update,
-//     combined graph) each fill the GPU, and two of them must never share it
-//     (each waits at grid barriers for all of its CTAs), so they run one at a
-//     time under a lock. An engine launch holds every SM's register file,
-//     so other kernels (another worker's Step 1) wait for it too; what
-//     overlaps with it is the other workers' host work (merging batches,
-//     change lists, result handling) and their host<->device copies.
+//   * overlap on the device: with W > 1 workers each worker's persistent
+//     cooperative launches (graph build, update, combined graph, costs) use
+//     at most SMs / W CTAs of one SM each, so the grids of W passes fit on
+//     the GPU side by side and run at the same time on disjoint SMs (each
+//     grid waits at its barriers only for its own CTAs). Full-grid work
+//     (adding a graph, or all passes when overlap is off) takes the engine
+//     lock exclusively; passes take it shared. Host work, copies and Step 1
+//     kernels of all workers overlap with the engine launches.
 // A response carries the graph's combined tree after the pass that included
 // the request and the version (number of batches applied to the graph) of
 // that state; equal versions give equal results however the batches were
@@ -36,8 +37,10 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <atomic>
 #include <memory>
 #include <mutex>
+#include <shared_mutex>
 #include <string>
 #include <thread>
 #include <unordered_map>
@@ -270,7 +273,12 @@ struct mosp_server {
   long long reserveBytes = 0;
   std::mutex mu;
   std::condition_variable workCv, doneCv;
-  std::mutex gpuLock;  // one persistent cooperative launch at a time
+  // shared by passes whose grids are limited to a worker's SM share,
+  // exclusive for full-grid launches
+  std::shared_mutex gpuLock;
+  bool overlap = true;   // passes of different workers run side by side
+  int workers = 1;
+  std::atomic<int> enginesActive{0};
   bool stop = false;
   int running = 0;
   std::vector<std::unique_ptr<Graph>> graphs;
@@ -521,7 +529,23 @@ int mosp_server::runPass(mosp_workspace *ws, cudaStream_t s, Staging &st, Graph 
   for (int k = 0; k < K; ++k) delta[k] = mosp_default_delta(g.m, n, g.weightSum[k]);
   const Clock::time_point tEngine = Clock::now();
   {
-    std::lock_guard<std::mutex> gpu(gpuLock);
+    std::shared_lock<std::shared_mutex> shared(gpuLock, std::defer_lock);
+    std::unique_lock<std::shared_mutex> whole(gpuLock, std::defer_lock);
+    // with overlap, this worker's share of the SMs for its cooperative
+    // grids, so that every worker's grids fit on the GPU together
+    const bool side = overlap && workers > 1;
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    mosp_workspace_set_grid(ws, side ? std::max(1, sms / workers) : 0, 0);
+    if (side) {
+      shared.lock();
+    } else {
+      whole.lock();
+    }
+    if (enginesActive.fetch_add(1) > 0) {
+      std::lock_guard<std::mutex> lk(mu);
+      ++stats.overlapped;
+    }
     rc = mosp_build_device_graph(ws, n, static_cast<int>(g.m), KG, g.row[g.cur], g.col[g.cur],
                                  g.w[g.cur], g.outW, g.inRow, g.inCol, g.inW, s);
     if (rc == MOSP_OK) {
@@ -531,6 +555,7 @@ int mosp_server::runPass(mosp_workspace *ws, cudaStream_t s, Staging &st, Graph 
                               g.maxWeight.data(), g.pref.empty() ? nullptr : g.pref.data(), g.dist,
                               g.parent, g.combDist, g.combParent, nullptr, nullptr, s);
     }
+    enginesActive.fetch_sub(1);
   }
   if (rc != MOSP_OK) {
     err = mosp_last_error();
@@ -578,6 +603,7 @@ void mosp_server::worker(int index) {
   Staging st;
   std::string setupErr;
   if (mosp_workspace_create(&ws) != MOSP_OK) setupErr = mosp_last_error();
+
   if (setupErr.empty() && cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
     setupErr = "stream creation failed";
   }
@@ -671,6 +697,7 @@ extern "C" int mosp_server_create(int workers, long long reserve_bytes, int max_
   }
   srv->reserveBytes = reserve_bytes;
   srv->maxCoalesce = max_coalesce;
+  srv->workers = workers;
   if (mosp_workspace_create(&srv->setupWs) != MOSP_OK) return MOSP_ERR_CUDA;
   if (cudaStreamCreateWithFlags(&srv->setupStream, cudaStreamNonBlocking) != cudaSuccess) {
     cudaGetLastError();
@@ -685,6 +712,13 @@ extern "C" int mosp_server_create(int workers, long long reserve_bytes, int max_
 }
 
 extern "C" void mosp_server_destroy(mosp_server *s) { delete s; }
+
+extern "C" int mosp_server_set_overlap(mosp_server *s, int on) {
+  if (s == nullptr || on < 0 || on > 1) return recordFailure(MOSP_ERR_INVALID, "Error: invalid overlap mode.");
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->overlap = on != 0;
+  return MOSP_OK;
+}
 
 extern "C" int mosp_server_add_graph(mosp_server *s, int n, int KG, int m, const int *h_row,
                                      const int *h_col, const int *h_w, int K, int source,
@@ -756,7 +790,7 @@ extern "C" int mosp_server_add_graph(mosp_server *s, int n, int KG, int m, const
   }
   {
     // initial canonical trees and the combined tree on the GPU
-    std::lock_guard<std::mutex> gpu(s->gpuLock);
+    std::unique_lock<std::shared_mutex> gpu(s->gpuLock);
     rc = mosp_build_device_graph(s->setupWs, n, m, KG, g->row[0], g->col[0], g->w[0], g->outW,
                                  g->inRow, g->inCol, g->inW, s->setupStream);
     for (int k = 0; k < K && rc == MOSP_OK; ++k) {

@@ -56,7 +56,7 @@ class ServerResult(C.Structure):
 class ServerStats(C.Structure):
     _fields_ = [("requests", C.c_longlong), ("passes", C.c_longlong), ("changes", C.c_longlong),
                 ("deferred", C.c_longlong), ("applies", C.c_longlong), ("max_coalesced", C.c_int),
-                ("reserved", C.c_int),
+                ("overlapped", C.c_int),
                 ("busy_us", C.c_double), ("apply_us", C.c_double), ("engine_us", C.c_double),
                 ("result_us", C.c_double)]
 
@@ -118,6 +118,7 @@ _SIGS = {
     "mosp_debug_barrier_cost": (_i, [_p, _i, _i, C.POINTER(C.c_double)]),
     "mosp_server_create": (_i, [_i, _ll, _i, C.POINTER(_p)]),
     "mosp_server_destroy": (None, [_p]),
+    "mosp_server_set_overlap": (_i, [_p, _i]),
     "mosp_server_add_graph": (_i, [_p, _i, _i, _i, _p, _p, _p, _i, _i, _ip, _ip]),
     "mosp_server_submit": (_i, [_p, _i, _i, _p, _p, _p, _i, _p, _p, _llp]),
     "mosp_server_wait": (_i, [_p, _ll, _p, _p, C.POINTER(ServerResult)]),
@@ -638,11 +639,12 @@ class Server:
     batches from any thread, coalesced per graph, admitted by free device
     memory."""
 
-    def __init__(self, workers=2, reserve_bytes=1 << 30, max_coalesce=64):
+    def __init__(self, workers=2, reserve_bytes=1 << 30, max_coalesce=64, overlap=True):
         h = C.c_void_p()
         check(lib().mosp_server_create(int(workers), int(reserve_bytes), int(max_coalesce), C.byref(h)))
         self._h = h
         self._n = {}
+        check(lib().mosp_server_set_overlap(self._h, 1 if overlap else 0))
 
     def close(self):
         if getattr(self, "_h", None) is not None:

@@ -94,7 +94,9 @@ def test_async_from_scratch(gpu, delta):
 def test_async_distance_only_fallback(gpu):
     """Weights near INT_MAX: distance-only words (the tag saturates) and the
     lowest-id parent recovery after the loop."""
-    row, col, w = grid_graph(40, 40, 2, 2 * 10 ** 9, 0.1, 36, wmin=10 ** 9)
+    # (n - 1) * maxWeight must exceed the 47 bits left next to a 17-bit
+    # parent field: 330 x 330 vertices with weights near INT_MAX
+    row, col, w = grid_graph(330, 330, 2, 2 * 10 ** 9, 0.1, 36, wmin=10 ** 9)
     g = mb.HostGraph.from_arrays(row, col, w)
     b = mb.HostBatch.generate(g, 300, seed=37, wmax=2 * 10 ** 9)
     ws = workspace(True)

@@ -147,3 +147,24 @@ def test_serving_rejects_bad_requests(scenario):
         assert info.version == 1 and np.array_equal(cd, states[0][1][2])
     finally:
         srv.close()
+
+
+def test_serving_passes_share_the_device(scenario):
+    """With several workers and overlap on, each worker's cooperative grids
+    use its share of the SMs, so passes of different graphs run on the
+    device at the same time; every response still equals the oracle (the
+    checks of serve()). The same requests with overlap off are served one
+    pass at a time and give the same results."""
+    st = serve(scenario, alone=False, workers=4)
+    assert st.passes <= st.requests
+    assert st.overlapped >= 1, "no two passes' engine launches ran at the same time"
+    K, graphs, prefs, batches, states = scenario
+    srv = mb.Server(workers=2, reserve_bytes=0, overlap=False)
+    try:
+        gid = srv.add_graph(graphs[2], K, 0, prefs[2])
+        for j, b in enumerate(batches[2]):
+            cd, cp, info = srv.wait(srv.submit(gid, b), gid)
+            assert np.array_equal(cd, states[2][info.version][2])
+        assert srv.stats().overlapped == 0
+    finally:
+        srv.close()
