@@ -282,6 +282,7 @@ struct StageHeader {
   u64 heavyD[kHeavyCap];       // push: the row's distance; pull: the word before the pass
   u64 heavyBest[kHeavyCap];    // pull: best word over the row, reduced by the CTA
   int asyncFar[kThreads / 32]; // async loop: entries in each warp's far buffer
+  int asyncLocal[kThreads / 32]; // async loop: entries in each warp's local buffer (may overshoot)
 };
 
 struct StageEntry {
@@ -431,13 +432,22 @@ constexpr int kSlots = MOSP_EDGE_SLOTS;
 constexpr unsigned long long kEmptySlot = ~0ULL;
 constexpr unsigned kTagSat = 0xFFFFFFFEu;  // distances >= this are not carried in the entry
 constexpr int kFarBuf = 128;               // per-warp far buffer entries (async loop)
+constexpr int kLocalBuf = 32;              // per-warp local near entries (async loop)
 constexpr int kWarps = kThreads / 32;
 
 struct AsyncState {
   AsyncShard *ctr;   // this phase's counter set
   int target;        // shard that receives this warp round's near entries
   unsigned spilled;  // this lane's reservations past the shard's capacity
+  bool local;        // near entries may stay in the warp's local buffer
 };
+
+/// Per-warp buffers of near entries the warp expands itself next (async
+/// loop), after the far buffers in the stage region.
+__device__ __forceinline__ u64 *asyncLocalBuffer(int warp) {
+  return reinterpret_cast<u64 *>(reinterpret_cast<int *>(stageEntries()) + kWarps * kFarBuf) +
+         warp * kLocalBuf;
+}
 
 /// Per-warp buffers of far-pile appends in the async loop (v << 5 | k), in
 /// the stage region of the dynamic shared memory.
@@ -501,15 +511,26 @@ __device__ __forceinline__ bool farBufferFull(int margin) {
 /// The active lanes share one reservation.
 __device__ __forceinline__ void asyncNear(const EngineParams &P, const LoopShared &L, AsyncState &A,
                                           int k, int w, u64 d) {
-  const unsigned mask = __activemask();
   const unsigned lane = laneId();
+  const unsigned tag = d < kTagSat ? static_cast<unsigned>(d) : kTagSat;
+  if (A.local) {
+    // the warp keeps up to kLocalBuf of its own pushes and expands them
+    // next, without the queue's round trips
+    const int warp = threadIdx.x >> 5;
+    const int slot = atomicAdd(&stageHeader().asyncLocal[warp], 1);
+    if (slot < kLocalBuf) {
+      asyncLocalBuffer(warp)[slot] =
+          (static_cast<u64>(tag) << 32) | ((static_cast<unsigned>(w) << 5) | static_cast<unsigned>(k));
+      return;
+    }
+  }
+  const unsigned mask = __activemask();
   const int leader = __ffs(mask) - 1;
   unsigned base = 0;
   if (static_cast<int>(lane) == leader) base = atomicAdd(&A.ctr[A.target].tail, __popc(mask));
   base = __shfl_sync(mask, base, leader);
   const unsigned idx = base + __popc(mask & ((1u << lane) - 1u));
   if (idx < P.aqShardCap) {
-    const unsigned tag = d < kTagSat ? static_cast<unsigned>(d) : kTagSat;
     const u64 e = (static_cast<u64>(tag) << 32) | ((static_cast<unsigned>(w) << 5) | static_cast<unsigned>(k));
     u64 *slot = P.aqSlots + static_cast<long long>(A.target) * P.aqShardCap + idx;
     // A consumer expands with min(tag, its read of the word), so only an
@@ -1051,9 +1072,40 @@ __device__ __forceinline__ void settleRound(AsyncShard *ctr, int from, unsigned 
   }
 }
 
-/// The consumer side of one phase for one warp: claim slots, expand the
-/// entries that arrive, until the phase is over (true) or the launch is
-/// stopped (false).
+/// Decode a near entry: objective k, vertex u (-1 if the entry is stale:
+/// a later, smaller distance has its own entry), the distance du to expand
+/// with and u's row. A word read older than the entry is covered by
+/// expanding with the entry's tag.
+template <int Mode>
+__device__ __forceinline__ void asyncEntry(const EngineParams &P, const int *outRow, u64 e, int &k,
+                                           int &u, u64 &du, int &beg, int &deg) {
+  const unsigned vk = static_cast<unsigned>(e);
+  const unsigned tag = static_cast<unsigned>(e >> 32);
+  k = static_cast<int>(vk & 31u);
+  const int v = static_cast<int>(vk >> 5);
+  const u64 word = __ldcg(P.packed + static_cast<long long>(k) * P.stride + v);
+  const int b0 = ldGraph<Mode>(outRow + v);
+  const int b1 = ldGraph<Mode>(outRow + v + 1);
+  const u64 d = word == kInfWord ? kInfWord : pkOf(P.obj[k]).dist(word);
+  u = -1;
+  if (tag < kTagSat) {
+    if (d >= tag) {
+      u = v;
+      du = tag;
+    }
+  } else if (d != kInfWord) {
+    u = v;
+    du = d;
+  }
+  if (u >= 0) {
+    beg = b0;
+    deg = b1 - b0;
+  }
+}
+
+/// The consumer side of one phase for one warp: expand its own local
+/// entries first, else claim slots and expand the entries that arrive,
+/// until the phase is over (true) or the launch is stopped (false).
 template <int Mode>
 __device__ bool asyncConsume(const EngineParams &P, const LoopShared &L, const int *outRow,
                              const int *outCol, const int *const *outWk, AsyncShard *ctr,
@@ -1066,7 +1118,36 @@ __device__ bool asyncConsume(const EngineParams &P, const LoopShared &L, const i
   int hops = 0;                          // shards found exhausted
   int target = static_cast<int>((gwarp * 7 + 3) % S);
   unsigned pend = 0, cb = 0, spins = 0;
+  // entries of shard cs consumed but not yet settled: a warp settles them
+  // only with its local buffer empty, so while it holds local work the
+  // shard's done stays below its tail and the phase cannot end
+  unsigned unsettled = 0;
+  StageHeader &H = stageHeader();
+  const int warp = threadIdx.x >> 5;
+  u64 *localBuf = asyncLocalBuffer(warp);
   while (true) {
+    __syncwarp();
+    int nLocal = __shfl_sync(kFull, H.asyncLocal[warp], 0);
+    if (nLocal > 0) {
+      nLocal = nLocal < kLocalBuf ? nLocal : kLocalBuf;
+      const u64 le = static_cast<int>(lane) < nLocal ? localBuf[lane] : kEmptySlot;
+      __syncwarp();
+      if (lane == 0) H.asyncLocal[warp] = 0;
+      __syncwarp();
+      int k = 0, u = -1, beg = 0, deg = 0;
+      u64 du = 0;
+      if (le != kEmptySlot) asyncEntry<Mode>(P, outRow, le, k, u, du, beg, deg);
+      AsyncState A{ctr, target, 0u, true};
+      expandWarp<Mode, true>(P, L, outRow, outCol, outWk, k, u, du, beg, deg, 0, nullptr, nullptr,
+                             false, &A);
+      settleRound(ctr, cs, 0u, target, A.spilled);
+      target = target + 1 == S ? 0 : target + 1;
+      continue;
+    }
+    if (unsettled != 0) {
+      settleRound(ctr, cs, unsettled, 0, 0u);
+      unsettled = 0;
+    }
     if (pend == 0 && hops < S) {
       unsigned b = 0;
       if (lane == 0) b = atomicAdd(&ctr[cs].head, 32u);
@@ -1115,34 +1196,13 @@ __device__ bool asyncConsume(const EngineParams &P, const LoopShared &L, const i
     u64 du = 0;
     if (e != kEmptySlot) {
       stRelaxed64(slot, kEmptySlot);
-      const unsigned vk = static_cast<unsigned>(e);
-      const unsigned tag = static_cast<unsigned>(e >> 32);
-      k = static_cast<int>(vk & 31u);
-      const int v = static_cast<int>(vk >> 5);
-      const u64 word = __ldcg(P.packed + static_cast<long long>(k) * P.stride + v);
-      const int b0 = ldGraph<Mode>(outRow + v);
-      const int b1 = ldGraph<Mode>(outRow + v + 1);
-      const u64 d = word == kInfWord ? kInfWord : pkOf(P.obj[k]).dist(word);
-      // stale (a later, smaller distance has its own entry) unless d >= tag;
-      // a word read older than the entry is covered by expanding with the tag
-      if (tag < kTagSat) {
-        if (d >= tag) {
-          u = v;
-          du = tag;
-        }
-      } else if (d != kInfWord) {
-        u = v;
-        du = d;
-      }
-      if (u >= 0) {
-        beg = b0;
-        deg = b1 - b0;
-      }
+      asyncEntry<Mode>(P, outRow, e, k, u, du, beg, deg);
     }
-    AsyncState A{ctr, target, 0u};
+    AsyncState A{ctr, target, 0u, true};
     expandWarp<Mode, true>(P, L, outRow, outCol, outWk, k, u, du, beg, deg, 0, nullptr, nullptr,
                            false, &A);
-    settleRound(ctr, cs, __popc(ready), target, A.spilled);
+    unsettled += __popc(ready);
+    settleRound(ctr, cs, 0u, target, A.spilled);
     target = target + 1 == S ? 0 : target + 1;
   }
 }
@@ -1169,7 +1229,10 @@ __device__ bool asyncNearFar(const EngineParams &P, const int *outRow, const int
     if (deltaOverride != nullptr && lane == 0) delta = *deltaOverride;
   }
   if (threadIdx.x < kMaxK) H.expanded[threadIdx.x] = 0;
-  if (threadIdx.x < kWarps) H.asyncFar[threadIdx.x] = 0;
+  if (threadIdx.x < kWarps) {
+    H.asyncFar[threadIdx.x] = 0;
+    H.asyncLocal[threadIdx.x] = 0;
+  }
   const unsigned long long t0 = globalNs();
   unsigned phase = 0;
   for (;; ++phase) {
@@ -1233,7 +1296,9 @@ __device__ bool asyncNearFar(const EngineParams &P, const int *outRow, const int
     // ---- split: this warp's share of the far piles, below the new
     // threshold to the near queue, the rest to the other pile
     {
-      AsyncState A{ctr, static_cast<int>(gwarp % S), 0u};
+      // (split pushes all go to the queue: a warp settles nothing in the
+      // split, so it must not hold local work past it)
+      AsyncState A{ctr, static_cast<int>(gwarp % S), 0u, false};
       for (long long base = gwarp * 32; base < total; base += nwarps * 32) {
         if (farBufferFull(32)) flushAsyncFar(P, L);
         const long long j = base + lane;
@@ -1529,7 +1594,8 @@ __device__ bool runNearFar(const EngineParams &P, const int *outRow, const int *
                            const int *const *outWk, Sync &epoch, u64 *deltaOverride, int genBase) {
   const bool async = (P.flags & kFlagAsync) != 0 && P.aqSlots != nullptr && P.aqShards > 0 &&
                      P.aqShards <= kAsyncShards && P.n <= (1 << 27) &&
-                     P.stageEntries * sizeof(StageEntry) >= kWarps * kFarBuf * sizeof(int) &&
+                     P.stageEntries * sizeof(StageEntry) >=
+                         kWarps * (kFarBuf * sizeof(int) + kLocalBuf * sizeof(u64)) &&
                      __ldcg(&P.ctl->heavy) == 0;
   if (async) return asyncNearFar<Mode>(P, outRow, outCol, outWk, epoch, deltaOverride, genBase);
   return nearFarLoop<Mode>(P, outRow, outCol, outWk, epoch, deltaOverride, genBase);
@@ -1568,6 +1634,59 @@ __device__ __forceinline__ u64 pullBest(const EngineParams &P, const ObjectiveAr
     }
   }
   return best;
+}
+
+/// The push direction of the pass before the near-far loop, for objective
+/// k: every valid (finite, not invalidated) vertex offers its distance plus
+/// the edge weight along each out-edge; strict improvements go to far pile
+/// 0 once (in-far flag). Warp gwarp of nwarps; a lane per short row, the
+/// whole warp per row of more than kLaneRowMax edges.
+__device__ void pushFromValid(const EngineParams &P, int k, const int *w, long long gwarp,
+                              long long nwarps) {
+  EngineControl *c = P.ctl;
+  const ObjectiveArgs &O = P.obj[k];
+  const Pk pk = pkOf(O);
+  const long long ko = static_cast<long long>(k) * P.stride;
+  const unsigned lane = laneId();
+  auto relax = [&](int u, u64 du, int e) {
+    const int x = __ldg(P.outCol + e);
+    const u64 nd = du + static_cast<u64>(__ldg(w + e));
+    if (x == P.source || nd > O.maxDist) return;
+    const u64 old = atomicMin(P.packed + ko + x, pk.pack(nd, u));
+    if (nd >= pk.dist(old)) return;
+    if (atomicExch(P.inFar + ko + x, 1) == 0) {
+      const int idx = warpAppend(&c->farCount[k][0]);
+      P.farL0[ko + idx] = x;
+      warpMinInto(&c->farMinC[k][0], nd);
+    }
+  };
+  for (long long base = gwarp * 32; base < P.n; base += nwarps * 32) {
+    const long long v = base + lane;
+    u64 word = kInfWord;
+    int beg = 0, end = 0;
+    if (v < P.n) {
+      word = __ldcg(P.packed + ko + v);
+      if (word != kInfWord) {
+        beg = __ldg(P.outRow + v);
+        end = __ldg(P.outRow + v + 1);
+      }
+    }
+    const u64 dv = word == kInfWord ? 0 : pk.dist(word);
+    const int deg = end - beg;
+    if (deg <= kLaneRowMax) {
+      for (int e = beg; e < end; ++e) relax(static_cast<int>(v), dv, e);
+    }
+    unsigned big = __ballot_sync(kFull, deg > kLaneRowMax);
+    while (big != 0) {
+      const int src = __ffs(big) - 1;
+      big &= big - 1;
+      const int ub = static_cast<int>(__shfl_sync(kFull, v, src));
+      const u64 db = __shfl_sync(kFull, dv, src);
+      const int bb = __shfl_sync(kFull, beg, src);
+      const int eb = __shfl_sync(kFull, end, src);
+      for (int e = bb + static_cast<int>(lane); e < eb; e += 32) relax(ub, db, e);
+    }
+  }
 }
 
 template <int Mode>
@@ -1750,11 +1869,25 @@ __global__ void __launch_bounds__(kThreads, 1) sospEngine(const __grid_constant_
     // ---- Pull pass over in-edges (reference :315-344) ----------------------
     // The improved candidates form far pile 0; the first iteration of the
     // loop sets the threshold to their minimum + delta and splits them.
+    //
+    // Direction per objective: when more than half of the vertices were
+    // invalidated, the few valid vertices push along all their out-edges
+    // instead (pushFromValid below). That makes the same offers to the
+    // invalidated vertices (their valid in-neighbours) and to the insert
+    // heads (every inserted edge leaves a valid or an invalidated vertex, and
+    // the latter is re-expanded in the loop anyway), for the out-edges of the
+    // valid part instead of the in-edges of the invalidated part.
+    __shared__ int sPush[kMaxK];
+    if (threadIdx.x < kMaxK) {
+      sPush[threadIdx.x] = static_cast<int>(threadIdx.x) < K && (P.flags & kFlagPullOnly) == 0 &&
+                           2LL * __ldcg(&c->invalidated[threadIdx.x]) > n;
+    }
+    __syncthreads();
     {
       __shared__ long long sOff[kMaxK + 1];
       if (warp == 0) {
         const long long cnt =
-            static_cast<int>(lane) < K ? __ldcg(&c->candCount[lane]) : 0;
+            static_cast<int>(lane) < K && !sPush[lane] ? __ldcg(&c->candCount[lane]) : 0;
         long long incl = cnt;
 #pragma unroll
         for (int off = 1; off < 32; off <<= 1) {
@@ -1935,6 +2068,9 @@ __global__ void __launch_bounds__(kThreads, 1) sospEngine(const __grid_constant_
         }
       }
       if (staged) flushPull();
+    }
+    for (int k = 0; k < K; ++k) {
+      if (sPush[k]) pushFromValid(P, k, sOutWk[k], tid >> 5, T >> 5);
     }
     if (!gridSync(c, epoch)) return;
     markPhase(c, kPhasePulled);

@@ -31,7 +31,7 @@ constexpr int kLaneRowMax = 32;               // rows above: warp-cooperative
 // entries of the per-CTA append stage of a bulk near-far launch (16 bytes
 // each, dynamic shared memory); asynchronous launches take fewer
 constexpr int kStageEntriesMax = MOSP_STAGE_ENTRIES;
-constexpr int kStageEntriesAsync = 1024;     // the far buffers of 32 warps
+constexpr int kStageEntriesAsync = 1536;     // far buffers + local buffers of 32 warps
 
 enum EngineMode : int { kModeUpdate = 0, kModeScratch = 1, kModeCombined = 2 };
 
@@ -98,9 +98,11 @@ enum : int {
   kFlagPrecheck = 1,     // read the word before the atomicMin of a relaxation
   kFlagHostRecovery = 2, // leave the lowest-id parent recovery of distance-only
                          // objectives to recoverParents, launched right after
-  kFlagAsync = 4         // asynchronous near-far loop (one grid barrier per far-pile
+  kFlagAsync = 4,        // asynchronous near-far loop (one grid barrier per far-pile
                          // split instead of one per iteration) when the graph has
                          // no hub rows
+  kFlagPullOnly = 8      // always pull into the candidates (never push from the
+                         // valid vertices)
 };
 
 /// Counters of one shard of the asynchronous near queue, each on its own
