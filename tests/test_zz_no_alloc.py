@@ -127,7 +127,7 @@ def test_static_distance_only_words(ws):
     recovery, through the static scratch, with tied distances."""
     row, col, w = grid_graph(60, 60, 1, 4, 0.1, 26)
     g, dg = upload(ws, row, col, w)
-    bound = 10 ** 12
+    bound = 10 ** 13
     for _ in range(2):
         ds, ps, st = static_tree(g, dg, 5, 3, bound)
         assert st.packed_parents == 0
