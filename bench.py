@@ -298,8 +298,9 @@ def run_ours(args):
     torch.cuda.synchronize()
     wall = time.perf_counter() - wall0
     clock = clocks.stop()
+    asy = ws.tuning()[2]
     phases = {"update": ws.last_phases(0), "combined": ws.last_phases(1),
-              "update_loop": ws.loop_profile(0), "combined_loop": ws.loop_profile(1)}
+              "update_loop": ws.loop_profile(0, asy), "combined_loop": ws.loop_profile(1, asy)}
     value, total_ms = replica_throughput(changed, args.steps, float(sum(step_ms)), world, pg, "cuda")
     if pg:
         pg.barrier()

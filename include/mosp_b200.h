@@ -415,8 +415,8 @@ int mosp_update_device(mosp_workspace *ws, int n, int m, int K,
 /* Autotuner of the near-far widths and local rounds: runs
  * mosp_update_device on the given inputs with the update width scaled by
  * 1/4 .. 8 around h_delta and 0..2 local rounds, and the combined-graph
- * width scaled by 1/2 .. 16 around its default with 0..4 local rounds,
- * timing each launch with CUDA events (best of two runs), and returns the
+ * width scaled by 1 .. 32 around its default with 0..4 local rounds,
+ * timing each launch with CUDA events (median of three runs), and returns the
  * fastest per-objective widths (h_best_delta, K entries), the fastest
  * combined width (*h_best_comb_delta, for
  * mosp_workspace_set_combined_delta), the fastest local rounds

@@ -1334,7 +1334,7 @@ int mosp_autotune_update(mosp_workspace *ws, int n, int m, int K, const int *d_o
     int rounds;
   };
   const Choice uc[] = {{1, 0}, {0.5, 0}, {2, 0}, {4, 0}, {1, 1}, {2, 1}, {0.25, 0}, {8, 0}, {2, 2}};
-  const Choice cc[] = {{1, 2}, {4, 2}, {16, 2}, {1, 0}, {4, 0}, {16, 0}, {4, 4}, {16, 4}, {8, 3}};
+  const Choice cc[] = {{1, 2}, {4, 2}, {16, 2}, {2, 0}, {8, 0}, {32, 0}, {4, 4}, {16, 4}, {8, 3}};
   const int trials = 9;
   float bestU = 1e30f, bestC = 1e30f;
   Choice bestUc = uc[0];
@@ -1348,8 +1348,9 @@ int mosp_autotune_update(mosp_workspace *ws, int n, int m, int K, const int *d_o
     ws->roundsUpdate = uc[t].rounds;
     ws->roundsScratch = cc[t].rounds;
     ws->combDelta = t == 0 ? 0 : std::max(1LL, static_cast<long long>(combDefault * cc[t].factor));
-    float u = 1e30f, c = 1e30f;
-    for (int rep = 0; rep < 2; ++rep) {
+    // median of three runs: sub-millisecond launches vary from run to run
+    float us[3], cs3[3];
+    for (int rep = 0; rep < 3; ++rep) {
       MOSP_CUDA(cudaMemcpyAsync(d_dist, saveDist, kn * sizeof(long long), cudaMemcpyDeviceToDevice, s));
       MOSP_CUDA(cudaMemcpyAsync(d_parent, saveParent, kn * sizeof(int), cudaMemcpyDeviceToDevice, s));
       mosp_combine_stats cs{};
@@ -1359,9 +1360,12 @@ int mosp_autotune_update(mosp_workspace *ws, int n, int m, int K, const int *d_o
                               d_dist, d_parent, d_comb_dist, d_comb_parent, nullptr, &cs, stream);
       if (st != MOSP_OK) return st;
       if (t == 0) combDefault = cs.delta;
-      u = std::min(u, ws->lastUpdateMs);
-      c = std::min(c, ws->lastCombinedMs);
+      us[rep] = ws->lastUpdateMs;
+      cs3[rep] = ws->lastCombinedMs;
     }
+    std::sort(us, us + 3);
+    std::sort(cs3, cs3 + 3);
+    const float u = us[1], c = cs3[1];
     if (u < bestU) {
       bestU = u;
       bestUc = uc[t];
@@ -1387,8 +1391,8 @@ int mosp_autotune_update(mosp_workspace *ws, int n, int m, int K, const int *d_o
     ws->roundsScratch = bestCr;
     ws->combDelta = bestComb;
     auto timeIt = [&](float &total) -> int {
-      total = 1e30f;
-      for (int rep = 0; rep < 2; ++rep) {
+      float runs[3];
+      for (int rep = 0; rep < 3; ++rep) {
         MOSP_CUDA(cudaMemcpyAsync(d_dist, saveDist, kn * sizeof(long long), cudaMemcpyDeviceToDevice, s));
         MOSP_CUDA(cudaMemcpyAsync(d_parent, saveParent, kn * sizeof(int), cudaMemcpyDeviceToDevice, s));
         const int rc = mosp_update_device(ws, n, m, K, d_out_row, d_out_col, d_out_w, d_in_row, d_in_col,
@@ -1397,8 +1401,10 @@ int mosp_autotune_update(mosp_workspace *ws, int n, int m, int K, const int *d_o
                                           h_pref, d_dist, d_parent, d_comb_dist, d_comb_parent, nullptr,
                                           nullptr, stream);
         if (rc != MOSP_OK) return rc;
-        total = std::min(total, ws->lastUpdateMs + ws->lastCombinedMs);
+        runs[rep] = ws->lastUpdateMs + ws->lastCombinedMs;
       }
+      std::sort(runs, runs + 3);
+      total = runs[1];
       return MOSP_OK;
     };
     struct Shape {

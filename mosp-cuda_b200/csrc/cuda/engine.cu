@@ -1106,10 +1106,16 @@ __device__ __forceinline__ void asyncEntry(const EngineParams &P, const int *out
 /// The consumer side of one phase for one warp: expand its own local
 /// entries first, else claim slots and expand the entries that arrive,
 /// until the phase is over (true) or the launch is stopped (false).
+/// Per-warp counters of the asynchronous loop (lane 0): rounds and entries
+/// taken from the queue and from the warp's local buffer.
+struct AsyncCounts {
+  long long queueRounds, localRounds, queueItems, localItems;
+};
+
 template <int Mode>
 __device__ bool asyncConsume(const EngineParams &P, const LoopShared &L, const int *outRow,
                              const int *outCol, const int *const *outWk, AsyncShard *ctr,
-                             unsigned phase, long long gwarp, const Sync &sync) {
+                             unsigned phase, long long gwarp, const Sync &sync, AsyncCounts &cnt) {
   EngineControl *c = P.ctl;
   const unsigned lane = laneId();
   const int S = P.aqShards;
@@ -1132,12 +1138,16 @@ __device__ bool asyncConsume(const EngineParams &P, const LoopShared &L, const i
       nLocal = nLocal < kLocalBuf ? nLocal : kLocalBuf;
       const u64 le = static_cast<int>(lane) < nLocal ? localBuf[lane] : kEmptySlot;
       __syncwarp();
-      if (lane == 0) H.asyncLocal[warp] = 0;
+      if (lane == 0) {
+        H.asyncLocal[warp] = 0;
+        ++cnt.localRounds;
+        cnt.localItems += nLocal;
+      }
       __syncwarp();
       int k = 0, u = -1, beg = 0, deg = 0;
       u64 du = 0;
       if (le != kEmptySlot) asyncEntry<Mode>(P, outRow, le, k, u, du, beg, deg);
-      AsyncState A{ctr, target, 0u, true};
+      AsyncState A{ctr, target, 0u, (P.flags & kFlagNoLocal) == 0};
       expandWarp<Mode, true>(P, L, outRow, outCol, outWk, k, u, du, beg, deg, 0, nullptr, nullptr,
                              false, &A);
       settleRound(ctr, cs, 0u, target, A.spilled);
@@ -1192,13 +1202,17 @@ __device__ bool asyncConsume(const EngineParams &P, const LoopShared &L, const i
     }
     spins = 0;
     pend &= ~ready;
+    if (lane == 0) {
+      ++cnt.queueRounds;
+      cnt.queueItems += __popc(ready);
+    }
     int k = 0, u = -1, beg = 0, deg = 0;
     u64 du = 0;
     if (e != kEmptySlot) {
       stRelaxed64(slot, kEmptySlot);
       asyncEntry<Mode>(P, outRow, e, k, u, du, beg, deg);
     }
-    AsyncState A{ctr, target, 0u, true};
+    AsyncState A{ctr, target, 0u, (P.flags & kFlagNoLocal) == 0};
     expandWarp<Mode, true>(P, L, outRow, outCol, outWk, k, u, du, beg, deg, 0, nullptr, nullptr,
                            false, &A);
     unsettled += __popc(ready);
@@ -1234,6 +1248,8 @@ __device__ bool asyncNearFar(const EngineParams &P, const int *outRow, const int
     H.asyncLocal[threadIdx.x] = 0;
   }
   const unsigned long long t0 = globalNs();
+  unsigned long long tPhase = t0;
+  AsyncCounts cnt{0, 0, 0, 0};
   unsigned phase = 0;
   for (;; ++phase) {
     if (threadIdx.x < kMaxK) H.farMin[threadIdx.x] = kInfWord;
@@ -1328,13 +1344,29 @@ __device__ bool asyncNearFar(const EngineParams &P, const int *outRow, const int
     }
 
     // ---- expand until the phase runs dry
-    if (!asyncConsume<Mode>(P, L, outRow, outCol, outWk, ctr, phase, gwarp, epoch)) return false;
+    if (!asyncConsume<Mode>(P, L, outRow, outCol, outWk, ctr, phase, gwarp, epoch, cnt)) return false;
     flushAsyncFar(P, L);
     __syncthreads();
     if (threadIdx.x < K && H.farMin[threadIdx.x] != kInfWord) {
       atomicMax(listTarget(P, L, K + threadIdx.x, 0, nullptr, nullptr).minC, ~H.farMin[threadIdx.x]);
     }
     if (!gridSync(c, epoch)) return false;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      // phase durations (the first four, then the rest summed)
+      const unsigned long long now = globalNs();
+      c->iterSplitNs[phase < 4 ? phase : 4] += now - tPhase;
+      tPhase = now;
+    }
+  }
+  if (lane == 0 && (cnt.queueRounds | cnt.localRounds) != 0) {
+    atomicAdd(reinterpret_cast<unsigned long long *>(&c->loopIters[1]),
+              static_cast<unsigned long long>(cnt.queueRounds + cnt.localRounds));
+    atomicAdd(reinterpret_cast<unsigned long long *>(&c->loopItems[0]),
+              static_cast<unsigned long long>(cnt.queueItems));
+    atomicAdd(reinterpret_cast<unsigned long long *>(&c->loopItems[1]),
+              static_cast<unsigned long long>(cnt.localItems));
+    atomicAdd(reinterpret_cast<unsigned long long *>(&c->loopNs[1]),
+              static_cast<unsigned long long>(cnt.localRounds));
   }
 
   if (threadIdx.x < K && H.expanded[threadIdx.x] != 0) {

@@ -82,14 +82,18 @@ struct alignas(128) EngineControl {
   long long pushes[kMaxK];
   // %globaltimer at the phase boundaries, written by CTA 0 (see kPhase*)
   unsigned long long phaseNs[8];
-  // near-far loop profile, written by CTA 0: time and items of iterations
-  // that split a far pile ([0]) and of pure push iterations ([1])
+  // near-far loop profile. Bulk loop (written by CTA 0): time and items of
+  // iterations that split a far pile ([0]) and of pure push iterations
+  // ([1]). Asynchronous loop: loopNs[0] its time, loopIters[0] its phases,
+  // loopIters[1] warp rounds, loopNs[1] of which local rounds, loopItems
+  // entries taken from the queue ([0]) and from local buffers ([1])
   unsigned long long loopNs[2];
   long long loopIters[2];
   long long loopItems[2];
-  // time (ns) of CTA 0 summed over the push iterations: decision step,
-  // thread 0's own items, waiting for the CTA's other warps, list flush,
-  // grid barrier
+  // bulk loop: time (ns) of CTA 0 summed over the push iterations: decision
+  // step, thread 0's own items, waiting for the CTA's other warps, list
+  // flush, grid barrier. Asynchronous loop: durations of phases 0-3 and of
+  // the rest
   unsigned long long iterSplitNs[5];
 };
 
@@ -101,8 +105,9 @@ enum : int {
   kFlagAsync = 4,        // asynchronous near-far loop (one grid barrier per far-pile
                          // split instead of one per iteration) when the graph has
                          // no hub rows
-  kFlagPullOnly = 8      // always pull into the candidates (never push from the
+  kFlagPullOnly = 8,     // always pull into the candidates (never push from the
                          // valid vertices)
+  kFlagNoLocal = 16      // asynchronous loop without warp-local continuation
 };
 
 /// Counters of one shard of the asynchronous near queue, each on its own

@@ -438,13 +438,21 @@ class Workspace:
                 prev = t
         return out
 
-    def loop_profile(self, which=0):
-        """Near-far loop of the last launch: {split|push: (ms, iterations,
-        items)}."""
+    def loop_profile(self, which=0, asynchronous=False):
+        """Near-far loop of the last launch. Bulk loop: {split|push: (ms,
+        iterations, items)} and the parts of a push iteration; asynchronous
+        loop: its time and phases, the durations of the first four phases
+        (the rest summed), warp rounds and the entries taken from the queue
+        and from the warps' local buffers."""
         ns = (C.c_ulonglong * 7)()
         it = (C.c_longlong * 2)()
         items = (C.c_longlong * 2)()
         check(lib().mosp_workspace_loop_profile(self._h, which, ns, it, items))
+        if asynchronous:
+            return {"ms": round(ns[0] / 1e6, 4), "phases": it[0],
+                    "phase_ms": [round(ns[2 + q] / 1e6, 4) for q in range(5)],
+                    "warp_rounds": it[1], "local_rounds": ns[1], "queue_entries": items[0],
+                    "local_entries": items[1]}
         out = {name: (round(ns[q] / 1e6, 4), it[q], items[q]) for q, name in enumerate(("split", "push"))}
         out["push_parts_ms"] = {name: round(ns[2 + q] / 1e6, 4) for q, name in
                                 enumerate(("decide", "own_items", "wait_cta", "flush", "barrier"))}
