@@ -1064,9 +1064,10 @@ __device__ __forceinline__ void settleRound(AsyncShard *ctr, int from, unsigned 
     for (int off = 16; off > 0; off >>= 1) spilled += __shfl_xor_sync(kFull, spilled, off);
   }
   if (consumed == 0 && spilled == 0) return;  // the same in every lane
+  // the warp barrier orders the lanes' reservations before lane 0's
+  // release adds, which order them (cumulatively) before the new counts
   __syncwarp();
   if (laneId() == 0) {
-    __threadfence();
     if (consumed != 0) redRelease(&ctr[from].done, consumed);
     if (spilled != 0) redRelease(&ctr[to].done, spilled);
   }
@@ -1147,7 +1148,7 @@ __device__ bool asyncConsume(const EngineParams &P, const LoopShared &L, const i
       int k = 0, u = -1, beg = 0, deg = 0;
       u64 du = 0;
       if (le != kEmptySlot) asyncEntry<Mode>(P, outRow, le, k, u, du, beg, deg);
-      AsyncState A{ctr, target, 0u, (P.flags & kFlagNoLocal) == 0};
+      AsyncState A{ctr, target, 0u, (P.flags & kFlagLocal) != 0};
       expandWarp<Mode, true>(P, L, outRow, outCol, outWk, k, u, du, beg, deg, 0, nullptr, nullptr,
                              false, &A);
       settleRound(ctr, cs, 0u, target, A.spilled);
@@ -1212,7 +1213,7 @@ __device__ bool asyncConsume(const EngineParams &P, const LoopShared &L, const i
       stRelaxed64(slot, kEmptySlot);
       asyncEntry<Mode>(P, outRow, e, k, u, du, beg, deg);
     }
-    AsyncState A{ctr, target, 0u, (P.flags & kFlagNoLocal) == 0};
+    AsyncState A{ctr, target, 0u, (P.flags & kFlagLocal) != 0};
     expandWarp<Mode, true>(P, L, outRow, outCol, outWk, k, u, du, beg, deg, 0, nullptr, nullptr,
                            false, &A);
     unsettled += __popc(ready);
@@ -1821,16 +1822,19 @@ __global__ void __launch_bounds__(kThreads, 1) sospEngine(const __grid_constant_
         for (int k = 0; k < K; ++k) {
           if (P.obj[k].nChanged == 0) continue;
           int *val = P.val + static_cast<long long>(k) * P.stride;
+          // up to four jumps per round, each along the pointers the other
+          // vertices have already lengthened, so a round covers more than
+          // twice the distance and fewer rounds (and full scans) are needed
           for (long long v = tid; v < n; v += T) {
-            const int a = __ldcg(val + v);
+            int a = __ldcg(val + v);
             if (a < 0) continue;
-            const int b = __ldcg(val + a);
-            if (b == -2 || b == -1) {
-              val[v] = b;
-            } else {
-              val[v] = b;
-              jumping = 1;
+            int b = __ldcg(val + a);
+            for (int hop = 1; hop < 4 && b >= 0; ++hop) {
+              a = b;
+              b = __ldcg(val + a);
             }
+            val[v] = b;
+            jumping |= b >= 0;
           }
         }
         if (__syncthreads_or(jumping) && threadIdx.x == 0) {

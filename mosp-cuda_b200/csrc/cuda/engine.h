@@ -107,7 +107,9 @@ enum : int {
                          // no hub rows
   kFlagPullOnly = 8,     // always pull into the candidates (never push from the
                          // valid vertices)
-  kFlagNoLocal = 16      // asynchronous loop without warp-local continuation
+  kFlagLocal = 16        // asynchronous loop with warp-local continuation (a warp
+                         // expands up to 32 of its own pushes next); measured
+                         // slower on the road workload (more re-expansions)
 };
 
 /// Counters of one shard of the asynchronous near queue, each on its own

@@ -178,3 +178,31 @@ def test_async_batched_roots(gpu):
         pe = np.where(pe >= 0, pe + off, pe)
         assert np.array_equal(res[0][1][off:off + pn], pe)
         off += pn
+
+
+def test_async_local_continuation_option(gpu, tmp_path):
+    """The opt-in warp-local continuation (engine switch 16, read from
+    MOSP_ENGINE_FLAGS when the library loads) reaches the same trees: run in
+    a fresh process with the switch set."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = """
+import sys
+sys.path[:0] = [{t!r}, {m!r}, {o!r}]
+import numpy as np
+import mosp_b200 as mb
+from conftest import grid_graph
+from gpu_util import assert_matches_oracle, run_update_device
+row, col, w = grid_graph(80, 70, 3, 100, 0.3, 77)
+g = mb.HostGraph.from_arrays(row, col, w)
+b = mb.HostBatch.generate(g, 1500, seed=78, wmax=100)
+ws = mb.Workspace(timeout_ms=20000)
+res = run_update_device(ws, g, b)
+assert_matches_oracle(res, g, b)
+print("LOCAL_OK")
+""".format(t=os.path.join(root, "tests"), m=os.path.join(root, "mosp-cuda_b200"), o=os.path.join(root, "oracle"))
+    env = dict(os.environ, MOSP_ENGINE_FLAGS="16")
+    out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0 and "LOCAL_OK" in out.stdout, out.stderr[-3000:]
