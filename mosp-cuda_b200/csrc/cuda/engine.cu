@@ -411,6 +411,13 @@ __device__ void flushStage(const EngineParams &P, const LoopShared &L, int wrSlo
 #define MOSP_EDGE_SLOTS 2
 #endif
 constexpr int kSlots = MOSP_EDGE_SLOTS;
+// asynchronous rounds: three slots per lane cover the ~90 edges of 32 road
+// vertices in one pass (one chain of edge loads, atomicMin and reservation
+// instead of two)
+#ifndef MOSP_EDGE_SLOTS_ASYNC
+#define MOSP_EDGE_SLOTS_ASYNC 3
+#endif
+constexpr int kSlotsAsync = MOSP_EDGE_SLOTS_ASYNC;
 
 // ---------------------------------------------------------------------------
 // Asynchronous near queue
@@ -688,17 +695,18 @@ __device__ __forceinline__ void expandWarp(const EngineParams &P, const LoopShar
   }
   const int edges = __shfl_sync(kFull, incl, 31);
   const int excl = incl - deg;
-  for (int s0 = 0; s0 < edges; s0 += 32 * kSlots) {
+  constexpr int SL = Async ? kSlotsAsync : kSlots;
+  for (int s0 = 0; s0 < edges; s0 += 32 * SL) {
     if constexpr (Async) {
       // room for this round's far appends in the warp's buffer
-      if (farBufferFull(32 * kSlots)) flushAsyncFar(P, L);
+      if (farBufferFull(32 * SL)) flushAsyncFar(P, L);
     }
-    // kSlots edge slots per lane, their loads and atomics overlapped
-    int sl[kSlots], kk[kSlots], uu[kSlots], ee[kSlots], ww[kSlots], wt[kSlots];
-    u64 dd[kSlots], nd[kSlots], old[kSlots];
-    bool act[kSlots];
+    // SL edge slots per lane, their loads and atomics overlapped
+    int sl[SL], kk[SL], uu[SL], ee[SL], ww[SL], wt[SL];
+    u64 dd[SL], nd[SL], old[SL];
+    bool act[SL];
 #pragma unroll
-    for (int h = 0; h < kSlots; ++h) {
+    for (int h = 0; h < SL; ++h) {
       sl[h] = s0 + 32 * h + static_cast<int>(lane);
       const int o = slotOwner(incl, sl[h]);
       kk[h] = __shfl_sync(kFull, k, o);
@@ -708,33 +716,33 @@ __device__ __forceinline__ void expandWarp(const EngineParams &P, const LoopShar
       act[h] = sl[h] < edges;
     }
 #pragma unroll
-    for (int h = 0; h < kSlots; ++h) {
+    for (int h = 0; h < SL; ++h) {
       ww[h] = act[h] ? ldGraph<Mode>(outCol + ee[h]) : 0;
       wt[h] = act[h] ? ldGraph<Mode>(outWk[kk[h]] + ee[h]) : 0;
     }
-    u64 cw[kSlots];
+    u64 cw[SL];
 #pragma unroll
-    for (int h = 0; h < kSlots; ++h) {
+    for (int h = 0; h < SL; ++h) {
       nd[h] = dd[h] + static_cast<u64>(wt[h]);
       act[h] = act[h] && ww[h] != P.source && nd[h] <= P.obj[kk[h]].maxDist;
       cw[h] = pkOf(P.obj[kk[h]]).pack(nd[h], uu[h]);
     }
     if (P.flags & kFlagPrecheck) {
-      u64 cur[kSlots];
+      u64 cur[SL];
 #pragma unroll
-      for (int h = 0; h < kSlots; ++h) {
+      for (int h = 0; h < SL; ++h) {
         cur[h] = act[h] ? __ldcg(P.packed + static_cast<long long>(kk[h]) * P.stride + ww[h]) : 0;
       }
 #pragma unroll
-      for (int h = 0; h < kSlots; ++h) act[h] = act[h] && cw[h] < cur[h];
+      for (int h = 0; h < SL; ++h) act[h] = act[h] && cw[h] < cur[h];
     }
 #pragma unroll
-    for (int h = 0; h < kSlots; ++h) {
+    for (int h = 0; h < SL; ++h) {
       old[h] = act[h] ? atomicMin(P.packed + static_cast<long long>(kk[h]) * P.stride + ww[h], cw[h])
                       : 0;
     }
 #pragma unroll
-    for (int h = 0; h < kSlots; ++h) {
+    for (int h = 0; h < SL; ++h) {
       if (!act[h] || nd[h] >= pkOf(P.obj[kk[h]]).dist(old[h])) continue;
       pushImproved<Async>(P, L, A, kk[h], ww[h], nd[h], wrSlot, nearWV, nearWD);
     }
@@ -1124,7 +1132,7 @@ __device__ bool asyncConsume(const EngineParams &P, const LoopShared &L, const i
   int cs = static_cast<int>(gwarp % S);  // shard this warp claims from
   int hops = 0;                          // shards found exhausted
   int target = static_cast<int>((gwarp * 7 + 3) % S);
-  unsigned pend = 0, cb = 0, spins = 0;
+  unsigned pend = 0, cb = 0, spins = 0, knownTail = 0;
   // entries of shard cs consumed but not yet settled: a warp settles them
   // only with its local buffer empty, so while it holds local work the
   // shard's done stays below its tail and the phase cannot end
@@ -1166,6 +1174,7 @@ __device__ bool asyncConsume(const EngineParams &P, const LoopShared &L, const i
       if (b >= cap) {
         cs = (cs + 1) % S;
         ++hops;
+        knownTail = 0;
         continue;
       }
       cb = b;
@@ -1174,12 +1183,16 @@ __device__ bool asyncConsume(const EngineParams &P, const LoopShared &L, const i
     }
     u64 *slot = P.aqSlots + static_cast<long long>(cs) * cap + cb + lane;
     u64 e = kEmptySlot;
-    // only slots below the shard's tail are reserved (one load per warp
-    // instead of 32 while the warp waits for work)
-    unsigned tail = 0;
-    if (pend != 0 && lane == 0) tail = ldVolatileU(&ctr[cs].tail);
-    tail = __shfl_sync(kFull, tail, 0);
-    if (((pend >> lane) & 1u) && cb + lane < tail) e = ldAcquire64(slot);
+    // only slots below the shard's tail are reserved; the tail only grows,
+    // so the last value read is reloaded only when a pending slot lies past
+    // it (one load per warp, and none while the shard is ahead of the warp)
+    const bool mine = (pend >> lane) & 1u;
+    if (__any_sync(kFull, mine && cb + lane >= knownTail)) {
+      unsigned t = 0;
+      if (lane == 0) t = ldVolatileU(&ctr[cs].tail);
+      knownTail = __shfl_sync(kFull, t, 0);
+    }
+    if (mine && cb + lane < knownTail) e = ldAcquire64(slot);
     const unsigned ready = __ballot_sync(kFull, e != kEmptySlot);
     if (ready == 0) {
       unsigned ph = 0;

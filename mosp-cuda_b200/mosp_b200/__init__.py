@@ -16,7 +16,9 @@ from dataclasses import dataclass
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libmosp_b200.so")
+# MOSP_B200_LIBRARY loads another build of the library (e.g. one compiled
+# with other build constants) in place of the in-tree one
+LIB_PATH = os.environ.get("MOSP_B200_LIBRARY") or os.path.join(os.path.dirname(_HERE), "lib", "libmosp_b200.so")
 BIN_DIR = os.path.join(os.path.dirname(_HERE), "bin")
 
 OK, ERR_INVALID, ERR_OVERFLOW, ERR_OOM, ERR_CUDA, ERR_TIMEOUT, ERR_UNSUPPORTED = range(7)
