@@ -129,6 +129,12 @@ void mosp_workspace_destroy(mosp_workspace *ws);
  * (no-op if large enough). */
 int mosp_workspace_reserve(mosp_workspace *ws, int n, int K);
 
+/* mosp_workspace_reserve plus everything the near-far loops of graphs with
+ * up to m edges need (near lists, the asynchronous near queue), so that
+ * later calls on such graphs allocate nothing in the workspace (e.g. a
+ * serving loop reserves before its first request). */
+int mosp_workspace_reserve_graph(mosp_workspace *ws, int n, long long m, int K);
+
 /* Batched instances: many independent graphs stored as one disjoint union
  * (vertex ids offset per instance) are updated by single launches when the
  * workspace knows every instance's root. After this call every entry point

@@ -786,6 +786,16 @@ int mosp_workspace_reserve(mosp_workspace *ws, int n, int K) {
   return reserveCombined(ws, std::max(n, 1), K);
 }
 
+int mosp_workspace_reserve_graph(mosp_workspace *ws, int n, long long m, int K) {
+  int st = mosp_workspace_reserve(ws, n, K);
+  if (st != MOSP_OK) return st;
+  if (m < 0) return fail(MOSP_ERR_INVALID, "invalid reserve size");
+  const long long nn = std::max(n, 1);
+  // the update's near lists and queue, and those of the combined step
+  if ((st = reserveNear(ws, nn, std::max(m, nn * K), K)) != MOSP_OK) return st;
+  return reserveAsync(ws, nn, K);
+}
+
 int mosp_workspace_set_sources(mosp_workspace *ws, const int *h_sources, int count) {
   int st = checkWorkspace(ws);
   if (st != MOSP_OK) return st;

@@ -278,6 +278,13 @@ struct mosp_server {
   std::shared_mutex gpuLock;
   bool overlap = true;   // passes of different workers run side by side
   int workers = 1;
+  // largest resident graph: every worker reserves its workspace and staging
+  // for it before its next pass (reserveEpoch counts the growths), so that
+  // passes allocate nothing - an allocation or free waits for the whole
+  // device, including the other workers' passes
+  int maxN = 0, maxK = 0;
+  long long maxM = 0;
+  int reserveEpoch = 0;
   std::atomic<int> enginesActive{0};
   bool stop = false;
   int running = 0;
@@ -607,15 +614,31 @@ void mosp_server::worker(int index) {
   if (setupErr.empty() && cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
     setupErr = "stream creation failed";
   }
+  int reservedEpoch = 0;
   for (;;) {
     std::unique_lock<std::mutex> lk(mu);
+    if (setupErr.empty() && reservedEpoch != reserveEpoch) {
+      const int n = maxN, K = maxK;
+      const long long m = maxM;
+      reservedEpoch = reserveEpoch;
+      lk.unlock();
+      std::string ignored;
+      // best effort: a pass that needs more still allocates what it needs
+      if (mosp_workspace_reserve_graph(ws, n, m + kPassChanges, K) == MOSP_OK) {
+        st.hostBytes(static_cast<long long>(n) * 12, ignored);
+      }
+      lk.lock();
+    }
     Graph *g = nullptr;
     workCv.wait(lk, [&] {
-      if (stop) return true;
+      if (stop || reservedEpoch != reserveEpoch) return true;
       g = pick();
       return g != nullptr;
     });
-    if (g == nullptr) break;  // stopping
+    if (g == nullptr) {
+      if (stop) break;
+      continue;  // reserve for a larger graph first
+    }
     std::vector<std::shared_ptr<Request>> group;
     // a pass takes up to maxCoalesce requests and, past its first request,
     // no more than kPassChanges changes, which bounds its duration
@@ -812,7 +835,14 @@ extern "C" int mosp_server_add_graph(mosp_server *s, int n, int KG, int m, const
   std::lock_guard<std::mutex> lk(s->mu);
   g->id = static_cast<int>(s->graphs.size());
   *graph_id = g->id;
+  if (n > s->maxN || m > s->maxM || K > s->maxK) {
+    s->maxN = std::max(s->maxN, n);
+    s->maxM = std::max<long long>(s->maxM, m);
+    s->maxK = std::max(s->maxK, K);
+    ++s->reserveEpoch;
+  }
   s->graphs.push_back(std::move(g));
+  s->workCv.notify_all();
   return MOSP_OK;
 }
 

@@ -78,6 +78,7 @@ _SIGS = {
     "mosp_workspace_create": (_i, [C.POINTER(_p)]),
     "mosp_workspace_destroy": (None, [_p]),
     "mosp_workspace_reserve": (_i, [_p, _i, _i]),
+    "mosp_workspace_reserve_graph": (_i, [_p, _i, _ll, _i]),
     "mosp_workspace_set_timeout_ms": (_i, [_p, _ll]),
     "mosp_workspace_set_ctas_per_sm": (_i, [_p, _i]),
     "mosp_workspace_set_sources": (_i, [_p, _ip, _i]),
