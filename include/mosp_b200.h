@@ -178,9 +178,10 @@ int mosp_workspace_set_narrow(mosp_workspace *ws, int max_items, int rounds);
  * than 2,048 edges; 0 runs the bulk-synchronous loop (one grid barrier per
  * iteration, the reference's schedule, src/sospUpdateGpu.cu:385-476) for
  * every graph. queue_slots bounds the near queue (8 bytes a slot; 0 = one
- * slot per vertex and objective plus n, at least 2^20): entries that find
- * it full go to the far pile and are taken up in the next phase. Results
- * do not depend on either. */
+ * slot per vertex and objective plus n, at least 2^20) and the bulk loop's
+ * near lists (entries per objective; 0 = min(n + m, max(2n, 2^20))):
+ * entries that find them full go to the far pile and are taken up in the
+ * next phase or split. Results do not depend on either. */
 int mosp_workspace_set_async(mosp_workspace *ws, int on, long long queue_slots);
 
 /* When on, mosp_update_device records its launch sequence (control-block

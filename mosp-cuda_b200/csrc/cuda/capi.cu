@@ -212,12 +212,20 @@ int ensureShape(mosp_workspace *ws) {
   return MOSP_OK;
 }
 
-/// Near lists of K objectives with room for n + m entries each: one
-/// iteration appends at most one entry per relaxation (<= m) and a split
-/// at most one per far-pile vertex (<= n).
+/// Near lists of K objectives (bulk loop). One iteration appends at most one
+/// entry per relaxation (<= m) and a split at most one per far-pile vertex
+/// (<= n), but the lists hold min(n + m, max(2n, 2^20)) + 64 entries each:
+/// appends past that go to the far pile (divertToFar), which the next split
+/// brings back, so the cap bounds memory without changing results.
 int reserveNear(mosp_workspace *ws, long long n, long long m, int K) {
-  const long long need = n + m + 64;
-  if (need <= ws->nearCap && K <= ws->nearK && ws->nearV0 != nullptr) return MOSP_OK;
+  long long need = std::min(n + m, std::max(2 * n, 1LL << 20)) + 64;
+  if (ws->asyncSlots > 0) {
+    // the caller's bound on the near queue caps the bulk loop's lists too
+    need = std::min(need, std::max(ws->asyncSlots, 1024LL));
+    if (need == ws->nearCap && K <= ws->nearK && ws->nearV0 != nullptr) return MOSP_OK;
+  } else if (need <= ws->nearCap && K <= ws->nearK && ws->nearV0 != nullptr) {
+    return MOSP_OK;
+  }
   const long long cap = std::max(need, ws->nearCap);
   const int kk = std::max(K, ws->nearK);
   releaseNear(ws);

@@ -338,6 +338,19 @@ __device__ __forceinline__ Target listTarget(const EngineParams &P, const LoopSh
                 &P.ctl->farMinC[k][s]};
 }
 
+/// A near entry (v, d) of objective k that found its near list full goes to
+/// the far pile instead (once, by the in-far flag); the split after the
+/// near list has run dry brings it back below the threshold. So the near
+/// lists can be smaller than the worst case of one iteration.
+__device__ __forceinline__ void divertToFar(const EngineParams &P, const LoopShared &L, int k, int v,
+                                            u64 d) {
+  if (atomicExch(P.inFar + static_cast<long long>(k) * P.stride + v, 1) != 0) return;
+  const Target t = listTarget(P, L, P.K + k, 0, nullptr, nullptr);
+  const int idx = warpAppend(t.counter);
+  t.v[idx] = v;
+  warpMinInto(t.minC, d);
+}
+
 /// Append (v, d) to list l (far lists: d only feeds the pile minimum). The
 /// staging buffer is split into one partition per list; the rank within the
 /// list is the slot, so a warp group needs one shared atomic.
@@ -369,6 +382,10 @@ __device__ __forceinline__ void stageAppend(const EngineParams &P, const LoopSha
     // partition full: this entry takes the direct global path
     const Target t = listTarget(P, L, l, wrSlot, nearWV, nearWD);
     const int idx = warpAppend(t.counter);
+    if (l < P.K && idx >= P.strideNear) {
+      divertToFar(P, L, l, v, d);
+      return;
+    }
     t.v[idx] = v;
     if (t.d != nullptr) t.d[idx] = d;
   }
@@ -400,6 +417,10 @@ __device__ void flushStage(const EngineParams &P, const LoopShared &L, int wrSlo
     const int b = H.base[l];
     for (int i = t; i < staged; i += blockDim.x) {
       const StageEntry e = E[l * H.cap + first + i];
+      if (l < K && b + i >= P.strideNear) {
+        divertToFar(P, L, l, e.v, e.d);  // the near list is full
+        continue;
+      }
       tg.v[b + i] = e.v;
       if (tg.d != nullptr) tg.d[b + i] = e.d;
     }
@@ -808,7 +829,9 @@ __device__ bool nearFarLoop(const EngineParams &P, const int *outRow,
       int mode = kDone;
       long long items = 0;
       if (act) {
-        const int nc = __ldcg(&c->nearCount[k][rdSlot]);
+        // (a count past the list's capacity counts entries diverted to far)
+        const int nc = static_cast<int>(
+            min(static_cast<long long>(__ldcg(&c->nearCount[k][rdSlot])), P.strideNear));
         if (nc > 0) {
           mode = kPush;
           items = nc;

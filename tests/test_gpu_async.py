@@ -206,3 +206,22 @@ print("LOCAL_OK")
     env = dict(os.environ, MOSP_ENGINE_FLAGS="16")
     out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600)
     assert out.returncode == 0 and "LOCAL_OK" in out.stdout, out.stderr[-3000:]
+
+
+def test_bulk_small_near_lists_overflow_to_far(gpu):
+    """The bulk loop with near lists of 1,024 entries per objective: appends
+    past them go to the far pile and come back at the next split; results
+    stay exact, for an update and from scratch."""
+    row, col, w = random_graph(4000, 16000, 3, 1000, 43)
+    g = mb.HostGraph.from_arrays(row, col, w)
+    b = mb.HostBatch.generate(g, 1500, seed=44, wmax=1000)
+    ws = workspace(False, queue_slots=1024)
+    res = run_update_device(ws, g, b)
+    assert_matches_oracle(res, g, b)
+    dg = mb.DeviceGraph.upload(ws, g)
+    d = torch.empty(g.n, dtype=torch.int64, device="cuda")
+    p = torch.empty(g.n, dtype=torch.int32, device="cuda")
+    ws.sosp_from_scratch(g.n, g.m, dg.out_row, dg.out_col, dg.out_w[:g.m], 3, 50, int(w.max()), d, p)
+    ws.close()
+    de, pe = orc.dijkstra(row, col, w, 0, 3)
+    assert np.array_equal(d.cpu().numpy(), de) and np.array_equal(p.cpu().numpy(), pe)
