@@ -67,7 +67,10 @@ def parse():
     ap.add_argument("--loop", choices=["auto", "async", "bulk"], default="auto",
                     help="near-far loop of the persistent launches: auto = the autotuner's choice "
                          "(results are the same)")
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the baselines: the CPU port and the reference's GPU binary")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip the reference's GPU binary (oracle/_ref/mosp_ref) beside the CPU baseline")
     ap.add_argument("--verify", action="store_true", help="check the result against the oracle")
     ap.add_argument("--requests", type=int, default=400, help="serving workload: requests per arrival rate")
     ap.add_argument("--rates", default="50,200,1000", help="serving workload: Poisson arrival rates (1/s)")
@@ -380,8 +383,12 @@ def run_ours(args):
         host_ws.close()
 
     cpu = None
+    ref_gpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_port(row, col, w, upd, ba, ch, old_d, old_p, K, src, changed, pref)
+        if not args.no_reference_gpu:
+            ref_gpu = reference_gpu_on(row, col, w, ba, [(old_d[k], old_p[k]) for k in range(K)], K, pref,
+                                       changed, local)
 
     if rank == 0:
         line = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -397,7 +404,7 @@ def run_ours(args):
                            "grid_ctas": grid_ctas, "hub_row_edges": hub_edges},
                 "gpu_compute_ms": round(ms_per_step, 4),
                 "default_widths_ms_per_step": round(float(np.mean(default_ms)), 4),
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "roofline": roofline, "cpu_baseline": cpu, "reference_gpu": ref_gpu, "e2e": e2e,
                 # update + combined launches, plus the parent-recovery kernel
                 # when an objective runs distance-only
                 "gpu_launches": (2 + (1 if any(s.packed_parents == 0 for s in stats) else 0)) * args.steps,
@@ -439,6 +446,92 @@ def cpu_baseline_port(row, col, w, upd, ba, ch, old_d, old_p, K, src, changed, p
     return {"value": round(changed / secs, 1), "unit": UNIT, "cores": 1, "kind": "port",
             "sample": f"one full MOSP update of the workload (K={K} sequential SOSP updates + host combined graph "
                       f"+ Dijkstra), compute only, {secs:.2f} s"}
+
+
+REF_MOSP = os.path.join(ROOT, "oracle", "_ref", "mosp_ref")
+
+
+def reference_gpu_on(row, col, w, batch, trees, K, pref, changed, device_index):
+    """reference_gpu_leg on the library arm's workload (original graph, batch
+    and initial trees written in the reference's formats to a temporary
+    directory), beside the CPU baseline."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    if not orc.have_ref() or not os.path.exists(REF_MOSP):
+        return {"unavailable": "oracle/_ref was not built (the reference sources were absent at build time)"}
+    tmp = tempfile.mkdtemp(prefix="mosp_refgpu_")
+    try:
+        prefix, changes, init = write_reference_inputs(tmp, row, col, w, batch, trees)
+        return reference_gpu_leg(prefix, changes, init, K, pref, changed, device_index=device_index)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+def write_reference_inputs(tmp, row, col, w, batch, trees):
+    """The workload as the reference's bin/mosp reads it (its own writers, from
+    oracle/_ref/libref_cpu.so): <tmp>/graph/graphCsr{RowPtr,ColInd,Values}.txt,
+    <tmp>/changes/{insert,delete}.txt and <tmp>/init/obj<k>/{distances
+    Original,SSSPTreeOriginal}.txt for the K (distance, parent) trees.
+    Returns (graph prefix, changes dir, init dir)."""
+    import oracle as orc
+    prefix = os.path.join(tmp, "graph", "graphCsr")
+    changes, init = os.path.join(tmp, "changes"), os.path.join(tmp, "init")
+    os.makedirs(os.path.dirname(prefix), exist_ok=True)
+    os.makedirs(changes, exist_ok=True)
+    orc.ref_write_csr(prefix, row, col, w)
+    orc.ref_write_changes(os.path.join(changes, "insert.txt"), os.path.join(changes, "delete.txt"),
+                          np.asarray(w).reshape(len(col), -1).shape[1], batch)
+    for k, (d, p) in enumerate(trees):
+        os.makedirs(os.path.join(init, f"obj{k}"), exist_ok=True)
+        orc.ref_write_tree(os.path.join(init, f"obj{k}", "distancesOriginal.txt"),
+                           os.path.join(init, f"obj{k}", "SSSPTreeOriginal.txt"), d, p)
+    return prefix, changes, init
+
+
+def reference_gpu_leg(prefix, changes, init, K, pref, changed, runs=5, device_index=0):
+    """The reference's own GPU path on the same B200: its bin/mosp, built from
+    its sources for sm_100a (oracle/_ref/mosp_ref), on the files of
+    write_reference_inputs, with its default bucket width. One untimed run
+    (which also writes the graph's binary cache), then `runs` runs, each its
+    own process; the figure is the median of the `RESULT gpu_compute_ms=`
+    each prints: the GPU work of the K SOSP updates plus the combined graph
+    and its SSSP, the region the reference times (src/mosp.cu:411).
+    Clocks are sampled over the runs."""
+    import re
+    if not os.path.exists(REF_MOSP):
+        return {"unavailable": "oracle/_ref/mosp_ref was not built (the reference sources were absent at build time)"}
+    cmd = [REF_MOSP, "--graph", prefix, "--changes", changes, "--init", init, "-k", str(K),
+           "--cache", prefix + ".cache", "--no-output", "--quiet"]
+    if pref is not None:
+        cmd += ["--pref", ",".join(str(int(x)) for x in pref)]
+    pat = re.compile(r"RESULT gpu_compute_ms=([0-9.]+) end_to_end_ms=([0-9.]+)")
+    sampler = ClockSampler(device_index)
+    compute, whole = [], []
+    failure = None
+    for i in range(runs + 1):
+        try:
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+        except subprocess.TimeoutExpired:
+            failure = "mosp_ref ran past 600 s"
+            break
+        found = pat.search(r.stdout)
+        if r.returncode != 0 or found is None:
+            tail = (r.stdout + r.stderr).strip().splitlines()[-1:] or [""]
+            failure = f"mosp_ref exited {r.returncode}: {tail[0][:200]}"
+            break
+        if i > 0:
+            compute.append(float(found.group(1)))
+            whole.append(float(found.group(2)))
+    clocks = sampler.stop()
+    if failure is not None:
+        return {"unavailable": failure}
+    ms = float(np.median(compute))
+    return {"value": round(changed / (ms / 1000.0), 1), "unit": UNIT, "gpu_compute_ms": round(ms, 3),
+            "gpu_compute_ms_runs": compute, "end_to_end_ms_median": round(float(np.median(whole)), 1),
+            "runs": len(compute), "clocks": clocks,
+            "what": "the reference's bin/mosp built from its sources for sm_100a (oracle/_ref/mosp_ref), default "
+                    "bucket width, --no-output; median RESULT gpu_compute_ms (K SOSP updates + combined graph + "
+                    "its SSSP); end_to_end_ms includes reading the text inputs"}
 
 
 # ---------------------------------------------------------------------------
@@ -697,6 +790,13 @@ def run_serving(args):
         def serve(workers, coalesce, paced):
             srv = mb.Server(workers=workers, reserve_bytes=4 << 30, max_coalesce=coalesce)
             ids = [srv.add_graph(ga, K, 0, pref) for ga in garrs]
+            # warm-up, not timed: one empty batch per graph (every worker has
+            # reserved its workspace for the largest graph by then)
+            empty = {"ins_from": np.zeros(0, np.int32), "ins_to": np.zeros(0, np.int32),
+                     "ins_w": np.zeros((0, K), np.int32), "del_from": np.zeros(0, np.int32),
+                     "del_to": np.zeros(0, np.int32)}
+            for gid in ids:
+                srv.wait(srv.submit(gid, empty), gid, want_result=False)
             infos = [None] * count
             tickets = [None] * count
             ready = threading.Semaphore(0)
@@ -826,20 +926,16 @@ def run_reference(args):
     m_upd = len(ucol)
     tmp = tempfile.mkdtemp(prefix="mosp_ref_")
     try:
-        prefix = os.path.join(tmp, "graph", "graphCsr")
-        os.makedirs(os.path.dirname(prefix))
-        orc.ref_write_csr(prefix, row, col, w)
-        ins, dele = os.path.join(tmp, "insert.txt"), os.path.join(tmp, "delete.txt")
-        orc.ref_write_changes(ins, dele, K, batch)
-        for k in range(K):
-            d, p = orc.ref_dijkstra(row, col, w, k, src)
-            orc.ref_write_tree(os.path.join(tmp, f"d{k}.txt"), os.path.join(tmp, f"t{k}.txt"), d, p)
+        trees = [orc.ref_dijkstra(row, col, w, k, src) for k in range(K)]
+        prefix, changes, init = write_reference_inputs(tmp, row, col, w, batch, trees)
+        ins, dele = os.path.join(changes, "insert.txt"), os.path.join(changes, "delete.txt")
 
         def objective(k):
             t0 = time.perf_counter()
-            ok, compute = orc.ref_sequential_update_timed(prefix, os.path.join(tmp, f"d{k}.txt"),
-                                                          os.path.join(tmp, f"t{k}.txt"), ins, dele, k, src,
-                                                          os.path.join(tmp, f"od{k}.txt"),
+            ok, compute = orc.ref_sequential_update_timed(prefix,
+                                                          os.path.join(init, f"obj{k}", "distancesOriginal.txt"),
+                                                          os.path.join(init, f"obj{k}", "SSSPTreeOriginal.txt"),
+                                                          ins, dele, k, src, os.path.join(tmp, f"od{k}.txt"),
                                                           os.path.join(tmp, f"ot{k}.txt"))
             whole = time.perf_counter() - t0
             if not ok:
@@ -874,6 +970,8 @@ def run_reference(args):
             list(pool.map(objective, range(K)))
         threaded = time.perf_counter() - t0 + comb_whole
 
+        ref_gpu = None if getattr(args, "no_reference_gpu", False) else reference_gpu_leg(prefix, changes, init, K, pref, changed)
+
         cores = os.cpu_count() or 1
         sample = (f"one objective's reference sequentialSOSPUpdate per step (file API: text graph, batch and tree "
                   f"read, batch applied, update, tree written; objective = step mod {K}), then once the "
@@ -897,6 +995,7 @@ def run_reference(args):
                 "threaded_variant": {"value": round(changed / threaded, 2), "unit": UNIT, "threads": K,
                                      "what": f"not the reference's behaviour: the {K} objectives in {K} threads at "
                                              "once, file API, plus the combined step"},
+                "reference_gpu": ref_gpu,
                 "host": {"cores": cores}}
         print(json.dumps(line), flush=True)
     finally:

@@ -3,6 +3,7 @@ configurations have the objective count, preferences, sizes and change
 batches their descriptions state, and the power-law options used for
 profiling captures change only the scale and the weight range."""
 import argparse
+import json
 
 import bench
 import mosp_b200 as mb
@@ -89,3 +90,7 @@ def test_reference_arm_loads_no_library_code():
     last = out.stdout.strip().splitlines()[-1]
     assert last == "CLEAN False", last
     assert '"impl": "reference"' in out.stdout
+    line = json.loads([x for x in out.stdout.splitlines() if x.startswith("{")][-1])
+    # the reference's GPU binary ran on the same files, or says why not
+    gpu = line["reference_gpu"]
+    assert ("unavailable" in gpu) or (gpu["runs"] == 5 and gpu["gpu_compute_ms"] > 0), gpu
