@@ -184,6 +184,19 @@ int mosp_workspace_set_narrow(mosp_workspace *ws, int max_items, int rounds);
  * next phase or split. Results do not depend on either. */
 int mosp_workspace_set_async(mosp_workspace *ws, int on, long long queue_slots);
 
+/* Declares that the input trees of this workspace's update calls follow the
+ * lowest-id tie rule (every tree this library returns does, and so does a
+ * tree from the reference's mospPrep init or canonicalizeTree). An
+ * objective that runs on distances alone (more than 64 bits per packed
+ * word) then recovers its parents only at the vertices the batch can reach
+ * (the vertices whose distance, parent distance or in-edges changed, and
+ * the out-neighbours of the vertices whose distance changed) instead of
+ * over every edge; for such input trees the result is the same. Off by
+ * default: the reference rebuilds every parent of such an objective
+ * (src/sospUpdateGpu.cu:491-512), which also normalises input trees that
+ * break ties differently. */
+int mosp_workspace_set_canonical_trees(mosp_workspace *ws, int on);
+
 /* When on, mosp_update_device records its launch sequence (control-block
  * clears, the update and combined launches, the status readback) as one
  * CUDA graph and replays it while the launch parameters stay the same; it

@@ -125,6 +125,15 @@ struct mosp_workspace {
   // narrow iterations (few items) run on one CTA with many local rounds
   int narrowItems = 512;
   int narrowRounds = 64;
+  // input trees declared canonical (mosp_workspace_set_canonical_trees):
+  // distance-only objectives recover parents only where the batch reaches;
+  // mark bytes (recMarkCap = K x n) and the list of long rows
+  bool canonicalTrees = false;
+  unsigned char *recMark = nullptr;
+  int *recVerts = nullptr;  // changed lists, then scan lists (2 x recMarkCap)
+  long long recMarkCap = 0;
+  u64 *recChunks = nullptr;  // two chunk lists of recChunkCap entries
+  long long recChunkCap = 0;
   // CUDA graph of mosp_update_device's launch sequence (mosp_workspace_use_graphs)
   bool useGraphs = false;
   cudaStream_t captureStream = nullptr;
@@ -390,6 +399,7 @@ void fillLists(EngineParams &p, mosp_workspace *ws, int block) {
   p.sources = ws->nSources > 1 ? ws->sources : nullptr;
   p.nSources = ws->nSources > 1 ? ws->nSources : 0;
   p.flags = engineFlags();
+  if (p.mode == kModeUpdate && p.recMark != nullptr) p.flags |= kFlagCanonical;
   p.heavyDeg = ws->heavyDeg;
   // asynchronous loop unless it is off or the graph last seen here had hub
   // rows; its launches need a smaller stage (the pull pass stays staged up
@@ -587,6 +597,31 @@ struct UpdateArgs {
 };
 
 /// Build the parameters of a fused K-objective update.
+/// Buffers of the restricted parent recovery: per objective and vertex of
+/// the engine lists one mark byte and two list slots (the changed and the
+/// scan list), and two chunk lists with room for every chunk of every row
+/// of more than kRecLightRow edges (at most m / kRecLightRow + 1 per
+/// objective).
+int reserveRecovery(mosp_workspace *ws, long long m, int K) {
+  int st = MOSP_OK;
+  const long long marks = ws->nCap * ws->kCap;
+  if (marks > ws->recMarkCap) {
+    ws->recMarkCap = 0;
+    // whole 32-bit words: the marks are set with atomicOr on their word
+    if ((st = deviceAlloc(&ws->recMark, (marks + 3) / 4 * 4)) != MOSP_OK) return st;
+    if ((st = deviceAlloc(&ws->recVerts, 2 * marks)) != MOSP_OK) return st;
+    ws->recMarkCap = marks;
+  }
+  const long long chunks = static_cast<long long>(K) * (m / kRecLightRow + 1) + 64;
+  if (chunks > INT_MAX) return fail(MOSP_ERR_INVALID, "Error: graph too large for the parent recovery lists.");
+  if (chunks > ws->recChunkCap) {
+    ws->recChunkCap = 0;
+    if ((st = deviceAlloc(&ws->recChunks, 2 * chunks)) != MOSP_OK) return st;
+    ws->recChunkCap = chunks;
+  }
+  return MOSP_OK;
+}
+
 int prepareUpdate(mosp_workspace *ws, const UpdateArgs &a, EngineParams &p, int *bitsOut) {
   if (a.n <= 0 || a.m < 0 || a.K < 1 || a.K > kMaxK || a.source < 0 || a.source >= a.n ||
       a.nHeads < 0 || (a.nHeads > 0 && a.heads == nullptr) || a.outRow == nullptr ||
@@ -631,6 +666,14 @@ int prepareUpdate(mosp_workspace *ws, const UpdateArgs &a, EngineParams &p, int 
     o.nChanged = a.nChanged[k];
     setObjective(o, bits, maxDist, a.delta[k]);
     bitsOut[k] = bits;
+  }
+  if (ws->canonicalTrees && std::any_of(bitsOut, bitsOut + a.K, [](int b) { return b == 0; })) {
+    if ((st = reserveRecovery(ws, a.m, a.K)) != MOSP_OK) return st;
+    p.recMark = ws->recMark;
+    p.recChangedList = ws->recVerts;
+    p.recScanList = ws->recVerts + ws->recMarkCap;
+    p.recChunkList = ws->recChunks;
+    p.recChunkCap = static_cast<int>(ws->recChunkCap);
   }
   return MOSP_OK;
 }
@@ -768,7 +811,8 @@ void mosp_workspace_destroy(mosp_workspace *ws) {
                   static_cast<void *>(ws->combW), static_cast<void *>(ws->cursor),
                   static_cast<void *>(ws->edgeOf), static_cast<void *>(ws->anc0),
                   static_cast<void *>(ws->anc1), static_cast<void *>(ws->acc0),
-                  static_cast<void *>(ws->acc1)}) {
+                  static_cast<void *>(ws->acc1), static_cast<void *>(ws->recMark),
+                  static_cast<void *>(ws->recVerts), static_cast<void *>(ws->recChunks)}) {
     if (p) cudaFree(p);
   }
   for (void *p : ws->user) {
@@ -859,6 +903,14 @@ int mosp_workspace_set_async(mosp_workspace *ws, int on, long long queue_slots) 
   }
   ws->asyncMode = on;
   ws->asyncSlots = queue_slots;
+  return MOSP_OK;
+}
+
+int mosp_workspace_set_canonical_trees(mosp_workspace *ws, int on) {
+  if (ws == nullptr || on < 0 || on > 1) {
+    return fail(MOSP_ERR_INVALID, "invalid canonical-trees setting");
+  }
+  ws->canonicalTrees = on != 0;
   return MOSP_OK;
 }
 

@@ -27,7 +27,10 @@
 //   * the lowest-id parent recovery of distance-only objectives is
 //     edge-balanced (equal edge slices per warp, a shuffle search for the
 //     rows) and, after an update launch, runs as its own kernel
-//     (recoverParents) so that L1 is not shared with the append stage.
+//     (recoverParents) so that L1 is not shared with the append stage;
+//     with input trees declared canonical it is restricted to the vertices
+//     the batch reaches (recover.cu: the unpack lists the vertices whose
+//     distance changed).
 //
 // Result semantics (identical to the reference): words pack
 // (distance << b | parent) and only strictly better words are kept
@@ -1519,6 +1522,9 @@ __device__ bool unpackResults(const EngineParams &P, const int *outRow,
   const int n = P.n, K = P.K;
   const long long tid = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   const long long T = static_cast<long long>(gridDim.x) * blockDim.x;
+  const bool restricted = Mode == kModeUpdate && P.recMark != nullptr && P.recChangedList != nullptr &&
+                          (P.flags & (kFlagCanonical | kFlagHostRecovery)) ==
+                              (kFlagCanonical | kFlagHostRecovery);
   bool anyFallback = false;
   for (int k = 0; k < K; ++k) {
     const ObjectiveArgs &O = P.obj[k];
@@ -1533,6 +1539,35 @@ __device__ bool unpackResults(const EngineParams &P, const int *outRow,
         } else {
           O.dist[v] = static_cast<long long>(pk.dist(word));
           O.parent[v] = pk.parent(word);
+        }
+      }
+    } else if (restricted) {
+      // restricted recovery (recover.cu): the input parents stay; the mark
+      // byte says whether the distance changed, and the changed vertices
+      // are listed (one reservation per warp)
+      anyFallback = true;
+      unsigned char *mark = P.recMark + ko;
+      int *changed = P.recChangedList + ko;
+      const int lane = static_cast<int>(laneId());
+      for (long long v0 = tid - lane; v0 < n; v0 += T) {  // the same v0 in the whole warp
+        const long long v = v0 + lane;
+        bool chg = false;
+        if (v < n) {
+          const u64 word = __ldcg(P.packed + ko + v);
+          const long long d = word == kInfWord ? kDistInf : static_cast<long long>(word);
+          chg = O.dist[v] != d;
+          mark[v] = chg ? kRecChanged : 0;
+          O.dist[v] = d;
+          if (word == kInfWord || isRoot(P.source, P.sources, P.nSources, static_cast<int>(v))) {
+            O.parent[v] = -1;
+          }
+        }
+        const unsigned bal = __ballot_sync(kFull, chg);
+        if (bal != 0) {
+          int at = 0;
+          if (lane == __ffs(bal) - 1) at = atomicAdd(&P.ctl->recChanged[k], __popc(bal));
+          at = __shfl_sync(kFull, at, __ffs(bal) - 1);
+          if (chg) changed[at + __popc(bal & ((1u << lane) - 1))] = static_cast<int>(v);
         }
       }
     } else {
@@ -2583,6 +2618,9 @@ cudaError_t launchRecovery(const EngineParams &p, cudaStream_t s) {
   cudaError_t err = cudaGetDevice(&device);
   if (err == cudaSuccess) err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   if (err != cudaSuccess) return err;
+  if ((p.flags & kFlagCanonical) != 0 && p.recMark != nullptr) {
+    return launchRestrictedRecovery(p, sms, s);
+  }
   recoverParents<<<sms * 8, 256, 0, s>>>(p);
   return cudaGetLastError();
 }

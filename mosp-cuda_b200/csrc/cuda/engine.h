@@ -95,6 +95,11 @@ struct alignas(128) EngineControl {
   // flush, grid barrier. Asynchronous loop: durations of phases 0-3 and of
   // the rest
   unsigned long long iterSplitNs[5];
+  // restricted parent recovery (kFlagCanonical): vertices in the changed
+  // and scan lists of each objective, and chunks in the two chunk lists
+  int recChanged[kMaxK];
+  int recScan[kMaxK];
+  int recChunks[2];
 };
 
 // EngineParams::flags (tuning switches; results do not depend on them)
@@ -107,10 +112,21 @@ enum : int {
                          // no hub rows
   kFlagPullOnly = 8,     // always pull into the candidates (never push from the
                          // valid vertices)
-  kFlagLocal = 16        // asynchronous loop with warp-local continuation (a warp
+  kFlagLocal = 16,       // asynchronous loop with warp-local continuation (a warp
                          // expands up to 32 of its own pushes next); measured
                          // slower on the road workload (more re-expansions)
+  kFlagCanonical = 32    // the input trees follow the lowest-id tie rule: with
+                         // kFlagHostRecovery, distance-only objectives recover
+                         // parents only where the batch can change them
+                         // (recover.cu); the same result as the full recovery
+                         // for such inputs
 };
+
+// Mark bytes of the restricted parent recovery (EngineParams::recMark, one
+// per objective and vertex): the update launch writes kRecChanged where a
+// distance-only objective's distance changed; kRecScan marks the vertices
+// whose in-row is scanned again.
+enum : unsigned char { kRecChanged = 1, kRecScan = 2 };
 
 /// Counters of one shard of the asynchronous near queue, each on its own
 /// 128-byte line: `head` is advanced by the warps that claim slots, `tail`
@@ -181,8 +197,27 @@ struct EngineParams {
   int combK, combBase;
   long long combDelta;         // > 0: fixed width; else default
   int prefTerms[kMaxK];        // L / Pref_i
+  // restricted parent recovery (kFlagCanonical): mark bytes [k * stride +
+  // v]; per objective the list of vertices whose distance changed
+  // (recChanged + k * stride) and of the other vertices whose in-row is
+  // scanned (recScanList + k * stride); chunks of rows of more than
+  // kRecLightRow edges: out-rows of changed vertices in [0, recChunkCap) of
+  // recChunkList, in-rows to scan in [recChunkCap, 2 recChunkCap)
+  unsigned char *recMark;
+  int *recChangedList;
+  int *recScanList;
+  u64 *recChunkList;
+  int recChunkCap;
   ObjectiveArgs obj[kMaxK];
 };
+static_assert(sizeof(EngineParams) <= 4096, "kernel parameter block limit");
+
+// rows of the restricted recovery up to this many edges are handled by the
+// warp of their vertex; longer rows go to a chunk list in chunks of
+// 2 kRecLightRow edges, one warp per chunk (so each chunk list needs at
+// most K (m / kRecLightRow + 1) entries, and no warp walks more than
+// 32 kRecLightRow edges of its own vertices)
+constexpr int kRecLightRow = 64;
 
 /// Parameters of the device-graph build.
 struct BuildParams {
@@ -227,8 +262,11 @@ cudaError_t launchEngineEx(const EngineParams &p, int ctas, cudaStream_t s);
 bool needsHostRecovery(const EngineParams &p);
 
 /// The lowest-id tight parent recovery of the distance-only objectives of
-/// update launch `p` (which ran with kFlagHostRecovery), on stream s.
+/// update launch `p` (which ran with kFlagHostRecovery), on stream s: over
+/// all edges, or (kFlagCanonical) only where the batch can change a parent.
 cudaError_t launchRecovery(const EngineParams &p, cudaStream_t s);
+/// The restricted recovery (recover.cu): four launches on stream s.
+cudaError_t launchRestrictedRecovery(const EngineParams &p, int sms, cudaStream_t s);
 cudaError_t launchBuild(const BuildParams &p, int ctas, cudaStream_t s);
 cudaError_t launchCosts(const CostParams &p, int ctas, cudaStream_t s);
 cudaError_t launchBarrierProbe(EngineControl *ctl, long long timeoutNs,

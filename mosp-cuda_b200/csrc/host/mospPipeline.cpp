@@ -499,6 +499,7 @@ bool mospUpdateWithCosts(const CsrGraph &original, ChangeBatch &batch,
     std::cerr << mosp_last_error() << "\n";
     return false;
   }
+  mosp_workspace_set_canonical_trees(ws, options.canonicalTrees ? 1 : 0);
   PipelineIn in;
   in.g = viewOf(original);
   in.b = viewOf(batch);

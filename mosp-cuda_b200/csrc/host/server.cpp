@@ -610,6 +610,9 @@ void mosp_server::worker(int index) {
   Staging st;
   std::string setupErr;
   if (mosp_workspace_create(&ws) != MOSP_OK) setupErr = mosp_last_error();
+  // every resident tree is this library's own output (canonical), so the
+  // distance-only objectives recover parents only where a pass reaches
+  if (setupErr.empty()) mosp_workspace_set_canonical_trees(ws, 1);
 
   if (setupErr.empty() && cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
     setupErr = "stream creation failed";

@@ -274,6 +274,8 @@ int main(int argc, char **argv) {
   options.numberOfObjectives = K;
   options.preferences = opt.pref;
   options.delta = opt.delta;
+  // trees normalised by --canonicalize follow the lowest-id rule
+  options.canonicalTrees = opt.canonicalize;
   CsrGraph updated;
   MospResult result;
   std::vector<long long> costs;

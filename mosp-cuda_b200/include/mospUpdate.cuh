@@ -19,6 +19,11 @@ struct MospOptions {
   int numberOfObjectives = 0;   ///< 0: every objective of the graph
   std::vector<int> preferences; ///< Pref vector; empty = all 1s
   long long delta = 0;          ///< near-far bucket width; <= 0: default
+  /// The initial trees follow the lowest-id tie rule (canonicalizeTree,
+  /// or any tree this library returns): distance-only objectives then
+  /// recover parents only where the batch reaches (same result for such
+  /// trees); see mosp_workspace_set_canonical_trees.
+  bool canonicalTrees = false;
 };
 
 /// Wall-clock times (milliseconds) of the stages of mospUpdate().

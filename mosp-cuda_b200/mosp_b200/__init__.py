@@ -87,6 +87,7 @@ _SIGS = {
     "mosp_workspace_set_local_rounds": (_i, [_p, _i, _i]),
     "mosp_workspace_set_narrow": (_i, [_p, _i, _i]),
     "mosp_workspace_set_async": (_i, [_p, _i, _ll]),
+    "mosp_workspace_set_canonical_trees": (_i, [_p, _i]),
     "mosp_workspace_set_grid": (_i, [_p, _i, _i]),
     "mosp_workspace_tuning": (_i, [_p, _ip, _ip, _ip]),
     "mosp_workspace_graph_launches": (_i, [_p, _ip]),
@@ -534,6 +535,12 @@ class Workspace:
         """Asynchronous near-far loop (default) or the bulk-synchronous one;
         queue_slots bounds the asynchronous near queue (0: default size)."""
         check(lib().mosp_workspace_set_async(self._h, 1 if on else 0, int(queue_slots)))
+
+    def set_canonical_trees(self, on=True):
+        """Declare that update inputs follow the lowest-id tie rule: the
+        distance-only objectives then recover parents only where the batch
+        reaches (same result for such trees)."""
+        check(lib().mosp_workspace_set_canonical_trees(self._h, 1 if on else 0))
 
     def use_graphs(self, on=True):
         check(lib().mosp_workspace_use_graphs(self._h, int(bool(on))))

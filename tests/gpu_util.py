@@ -24,10 +24,12 @@ def initial_trees(graph_arrays, K, source=0):
     return d, p
 
 
-def run_update_device(ws, g, batch, K=None, source=0, pref=None, init=None, delta=None):
+def run_update_device(ws, g, batch, K=None, source=0, pref=None, init=None, delta=None, max_weight=None):
     """One MOSP update through mosp_update_device: the batch is applied by
     the library (host), the updated graph uploaded, the K fused updates and
-    Steps 2-3 run on the GPU. Returns numpy results and the stats."""
+    Steps 2-3 run on the GPU. Returns numpy results and the stats.
+    max_weight overrides the per-objective weight bound (a larger bound
+    makes the objectives run distance-only)."""
     K = K or g.K
     ga = g.arrays()
     d0, p0 = init if init is not None else initial_trees(ga, K, source)
@@ -42,6 +44,8 @@ def run_update_device(ws, g, batch, K=None, source=0, pref=None, init=None, delt
     orig_w = ga[2]
     maxw = [max(1, int(orig_w[:, k].max()) if len(orig_w) else 1,
                 int(ba["ins_w"][:, k].max()) if len(ba["ins_w"]) else 1) for k in range(K)]
+    if max_weight is not None:
+        maxw = [int(max_weight)] * K
     if delta is None:
         deltas = [mb.default_delta(max(g.m, 1), g.n, int(orig_w[:, k].sum())) for k in range(K)]
     else:

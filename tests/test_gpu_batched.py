@@ -84,7 +84,24 @@ def run_union(ws, insts, K=3):
 
 @pytest.mark.parametrize("count,seed", [(2, 41), (12, 42), (40, 43)])
 def test_batched_update_equals_each_instance(ws, count, seed):
-    insts = instances(count, seed)
+    check_each_instance(ws, instances(count, seed))
+
+
+def test_batched_workload_full_size(ws):
+    """The benchmark's batched workload at full size: 256 grid-road
+    instances of 1,000 to 200,000 vertices, each with its own batch of 1-10%
+    of its edges in one of four modes, in one union; every instance equals
+    the oracle run on that instance alone."""
+    import bench
+    insts = []
+    for g, b, _ in bench.make_batched_workload(256):
+        ba = b.arrays()
+        insts.append((g.arrays(), {k: ba[k] for k in ("ins_from", "ins_to", "ins_w", "del_from", "del_to")}))
+    assert len(insts) == 256
+    check_each_instance(ws, insts)
+
+
+def check_each_instance(ws, insts):
     off, dist, par, cd, cp, costs, cst = run_union(ws, insts)
     edges = 0
     for i, (g, b) in enumerate(insts):

@@ -36,12 +36,13 @@ def initial_trees_gpu(ws, g, K):
     return d.cpu().numpy(), p.cpu().numpy()
 
 
-def check_full(ws, g, batch, K, pref):
+def check_full(ws, g, batch, K, pref, exp=None):
     d0, p0 = initial_trees_gpu(ws, g, K)
     garr = g.arrays()
     ba = batch.arrays()
     dist, par, cd, cp, costs, _ = ws.update_host(garr, ba, d0, p0, K, 0, pref=pref, costs=True)
-    exp = orc.expected_update(garr, ba, K, 0, pref)
+    if exp is None:
+        exp = orc.expected_update(garr, ba, K, 0, pref)
     for k in range(K):
         assert np.array_equal(dist[k], exp["dist"][k]), k
         assert np.array_equal(par[k], exp["parent"][k]), k
@@ -65,4 +66,11 @@ def test_power_law_fallback_full_size(ws):
     # (n - 1) * maxWeight does not fit next to 23 parent bits: the
     # distance-only words with lowest-id parent recovery run
     assert mb.choose_packing(g.n, 1_000_000)[0] == 0
-    check_full(ws, g, b, 5, [1, 2, 3, 4, 5])
+    exp = check_full(ws, g, b, 5, [1, 2, 3, 4, 5])
+    # the initial trees are the library's own (canonical): the recovery
+    # restricted to what the batch reaches gives the same trees
+    ws.set_canonical_trees(True)
+    try:
+        check_full(ws, g, b, 5, [1, 2, 3, 4, 5], exp=exp)
+    finally:
+        ws.set_canonical_trees(False)
