@@ -11,8 +11,9 @@ For canonical input trees (the oracle's lowest-id Dijkstra trees here) both
 must give the oracle's trees bit for bit. The weight bound passed to the
 library is raised so that every objective runs distance-only, and weights
 in 1..3 make ties everywhere. Covered: every batch kind, both near-far
-loops, rows of more than 512 edges in both directions (the listed rows,
-handled in chunks by whole CTAs), batched roots, and an empty batch."""
+loops, rows of more than 64 edges in both directions (the listed rows,
+handled in 128-edge chunks, one warp per chunk), batched roots, repeated
+updates and an empty batch."""
 import numpy as np
 import pytest
 
