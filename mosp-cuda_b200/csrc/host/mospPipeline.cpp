@@ -107,10 +107,11 @@ bool syncStream(cudaStream_t s, std::string &err) {
 
 /// The pipeline's two streams (per host thread): the main stream runs the
 /// batch upload, Step 1 and the engine; the side stream moves the trees
-/// (upload while Step 1 runs, download while the combined step runs).
+/// (upload while Step 1 runs, the K trees' download while the combined step
+/// runs, the combined tree's while the path costs run).
 struct PipelineStreams {
   cudaStream_t main = nullptr, side = nullptr;
-  cudaEvent_t treesIn = nullptr, updated = nullptr;
+  cudaEvent_t treesIn = nullptr, updated = nullptr, combined = nullptr;
   int device = -1;
   ~PipelineStreams() { release(); }
   void release() {
@@ -120,9 +121,10 @@ struct PipelineStreams {
     cudaSetDevice(device);
     if (treesIn) cudaEventDestroy(treesIn);
     if (updated) cudaEventDestroy(updated);
+    if (combined) cudaEventDestroy(combined);
     if (main) cudaStreamDestroy(main);
     if (side) cudaStreamDestroy(side);
-    treesIn = updated = nullptr;
+    treesIn = updated = combined = nullptr;
     main = side = nullptr;
     device = -1;
     if (current >= 0) cudaSetDevice(current);
@@ -137,7 +139,8 @@ struct PipelineStreams {
     if (cudaStreamCreateWithFlags(&main, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&treesIn, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&updated, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&updated, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&combined, cudaEventDisableTiming) != cudaSuccess) {
       cudaGetLastError();
       err = "Error: stream creation failed.";
       return false;
@@ -399,6 +402,14 @@ int runPipeline(mosp_workspace *ws, const PipelineIn &in, PipelineOut &out, std:
     }
   }
   out.t.combined = msSince(t0);
+  // the combined tree goes back on the side stream while the costs run
+  if (cudaEventRecord(streams.combined, sm) != cudaSuccess ||
+      cudaStreamWaitEvent(ss, streams.combined, 0) != cudaSuccess ||
+      !toHostAsync(out.combDist, dCombDist, static_cast<size_t>(n), ss, err) ||
+      !toHostAsync(out.combParent, dCombParent, static_cast<size_t>(n), ss, err)) {
+    if (err.empty()) err = "Error: stream wait failed.";
+    return MOSP_ERR_CUDA;
+  }
 
   if (in.costs) {
     t0 = std::chrono::steady_clock::now();
@@ -416,9 +427,7 @@ int runPipeline(mosp_workspace *ws, const PipelineIn &in, PipelineOut &out, std:
   t0 = std::chrono::steady_clock::now();
   {
     ScopedStage stage("download", true);
-    if (!toHostAsync(out.combDist, dCombDist, static_cast<size_t>(n), sm, err) ||
-        !toHostAsync(out.combParent, dCombParent, static_cast<size_t>(n), sm, err) ||
-        (in.costs && !toHostAsync(out.costs, dCosts, static_cast<size_t>(n) * KG, sm, err)) ||
+    if ((in.costs && !toHostAsync(out.costs, dCosts, static_cast<size_t>(n) * KG, sm, err)) ||
         !syncStream(sm, err) || !syncStream(ss, err)) {
       return MOSP_ERR_CUDA;
     }
