@@ -1896,16 +1896,33 @@ __global__ void __launch_bounds__(kThreads, 1) sospEngine(const __grid_constant_
           // up to four jumps per round, each along the pointers the other
           // vertices have already lengthened, so a round covers more than
           // twice the distance and fewer rounds (and full scans) are needed
-          for (long long v = tid; v < n; v += T) {
-            int a = __ldcg(val + v);
-            if (a < 0) continue;
-            int b = __ldcg(val + a);
-            for (int hop = 1; hop < 4 && b >= 0; ++hop) {
-              a = b;
-              b = __ldcg(val + a);
+          // four vertices per thread (v, v + T, v + 2T, v + 3T) with their
+          // chains of dependent loads in flight together
+          for (long long v0 = tid; v0 < n; v0 += 4 * T) {
+            int a[4], b[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const long long v = v0 + q * T;
+              a[q] = v < n ? __ldcg(val + v) : -1;
             }
-            val[v] = b;
-            jumping |= b >= 0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) b[q] = a[q] >= 0 ? __ldcg(val + a[q]) : -1;
+#pragma unroll
+            for (int hop = 1; hop < 4; ++hop) {
+#pragma unroll
+              for (int q = 0; q < 4; ++q) {
+                if (a[q] >= 0 && b[q] >= 0) {
+                  a[q] = b[q];
+                  b[q] = __ldcg(val + a[q]);
+                }
+              }
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              if (a[q] < 0) continue;  // no ancestor pointer (or past n)
+              val[v0 + q * T] = b[q];
+              jumping |= b[q] >= 0;
+            }
           }
         }
         if (__syncthreads_or(jumping) && threadIdx.x == 0) {
