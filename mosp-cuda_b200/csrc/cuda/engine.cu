@@ -1531,14 +1531,25 @@ __device__ bool unpackResults(const EngineParams &P, const int *outRow,
     const Pk pk = pkOf(O);
     const long long ko = static_cast<long long>(k) * P.stride;
     if (O.parentBits > 0) {
-      for (long long v = tid; v < n; v += T) {
-        const u64 word = __ldcg(P.packed + ko + v);
-        if (word == kInfWord) {
-          O.dist[v] = kDistInf;
-          O.parent[v] = -1;
-        } else {
-          O.dist[v] = static_cast<long long>(pk.dist(word));
-          O.parent[v] = pk.parent(word);
+      // four words per thread (v, v + T, v + 2T, v + 3T), loaded together
+      for (long long v0 = tid; v0 < n; v0 += 4 * T) {
+        u64 word[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const long long v = v0 + q * T;
+          word[q] = v < n ? __ldcg(P.packed + ko + v) : kInfWord;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const long long v = v0 + q * T;
+          if (v >= n) break;
+          if (word[q] == kInfWord) {
+            O.dist[v] = kDistInf;
+            O.parent[v] = -1;
+          } else {
+            O.dist[v] = static_cast<long long>(pk.dist(word[q]));
+            O.parent[v] = pk.parent(word[q]);
+          }
         }
       }
     } else if (restricted) {
@@ -1826,37 +1837,53 @@ __global__ void __launch_bounds__(kThreads, 1) sospEngine(const __grid_constant_
   if constexpr (Mode == kModeUpdate) {
     // ---- Heavy rows: does the graph have rows for whole-CTA handling? -----
     const int heavyDeg = heavyDegOf(P);
+    bool heavyRow = false;  // one store at the end, so the loads run ahead
     for (long long v = tid; v < n; v += T) {
-      if (__ldg(outRow + v + 1) - __ldg(outRow + v) > heavyDeg ||
-          __ldg(P.inRow + v + 1) - __ldg(P.inRow + v) > heavyDeg) {
-        c->heavy = 1;
-      }
+      heavyRow |= __ldg(outRow + v + 1) - __ldg(outRow + v) > heavyDeg ||
+                  __ldg(P.inRow + v + 1) - __ldg(P.inRow + v) > heavyDeg;
     }
+    if (heavyRow) c->heavy = 1;
     // ---- Pack the old trees; ancestors (reference :234-252) ---------------
+    // four vertices per thread (v, v + T, v + 2T, v + 3T): their loads are
+    // issued before any of their stores
+    bool badParent = false, badDist = false;
     for (int k = 0; k < K; ++k) {
       const ObjectiveArgs &O = P.obj[k];
       const Pk pk = pkOf(O);
       const long long ko = static_cast<long long>(k) * P.stride;
-      for (long long v = tid; v < n; v += T) {
-        const long long d = O.dist[v];
-        int p = O.parent[v];
-        if (p < -1 || p >= n) {
-          c->invalid = 1;
-          p = -1;
+      for (long long v0 = tid; v0 < n; v0 += 4 * T) {
+        long long d[4];
+        int p[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const long long v = v0 + q * T;
+          d[q] = v < n ? O.dist[v] : kDistInf;
+          p[q] = v < n ? O.parent[v] : -1;
         }
-        u64 word;
-        if (d >= kDistInf / 2) {
-          word = kInfWord;
-        } else if (d < 0 || static_cast<u64>(d) > O.maxDist) {
-          c->overflow = 1;
-          word = kInfWord;
-        } else {
-          word = pk.pack(static_cast<u64>(d), p);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const long long v = v0 + q * T;
+          if (v >= n) break;
+          if (p[q] < -1 || p[q] >= n) {
+            badParent = true;
+            p[q] = -1;
+          }
+          u64 word;
+          if (d[q] >= kDistInf / 2) {
+            word = kInfWord;
+          } else if (d[q] < 0 || static_cast<u64>(d[q]) > O.maxDist) {
+            badDist = true;
+            word = kInfWord;
+          } else {
+            word = pk.pack(static_cast<u64>(d[q]), p[q]);
+          }
+          P.packed[ko + v] = word;
+          P.val[ko + v] = p[q];  // >= 0: ancestor; -1: none; -2: invalidated
         }
-        P.packed[ko + v] = word;
-        P.val[ko + v] = p;  // >= 0: ancestor; -1: none; -2: invalidated
       }
     }
+    if (badParent) c->invalid = 1;
+    if (badDist) c->overflow = 1;
     if (!gridSync(c, epoch)) return;
     markPhase(c, kPhasePacked);
 
