@@ -2253,22 +2253,30 @@ __device__ void scratchOrCombined(const EngineParams &P, Sync &epoch, int genBas
     // src/combinedGraphGpu.cu:80-121, 281-300), then Step 3 below --------
     for (long long v = tid; v <= n; v += T) P.combDeg[v] = 0;
     if (!gridSync(c, epoch)) return;
+    // four vertices per thread (v, v + T, v + 2T, v + 3T) in the count and
+    // fill passes, so their parent loads and atomics are in flight together
     unsigned long long edges = 0, wsum = 0;
-    for (long long v = tid; v < n; v += T) {
-      if (isRoot(P.source, P.sources, P.nSources, static_cast<int>(v))) continue;
-      for (int k = 0; k < P.combK; ++k) {
-        int p, w;
-        if (combinedEdge(P, static_cast<int>(v), k, p, w)) {
-          if (p >= n) {
-            c->invalid = 1;
-            continue;
+    bool badParent = false;
+    for (long long v0 = tid; v0 < n; v0 += 4 * T) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const long long v = v0 + q * T;
+        if (v >= n || isRoot(P.source, P.sources, P.nSources, static_cast<int>(v))) continue;
+        for (int k = 0; k < P.combK; ++k) {
+          int p, w;
+          if (combinedEdge(P, static_cast<int>(v), k, p, w)) {
+            if (p >= n) {
+              badParent = true;
+              continue;
+            }
+            atomicAdd(P.combDeg + p, 1);
+            ++edges;
+            wsum += static_cast<unsigned long long>(w);
           }
-          atomicAdd(P.combDeg + p, 1);
-          ++edges;
-          wsum += static_cast<unsigned long long>(w);
         }
       }
     }
+    if (badParent) c->invalid = 1;
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
       edges += __shfl_down_sync(kFull, edges, off);
@@ -2288,14 +2296,18 @@ __device__ void scratchOrCombined(const EngineParams &P, Sync &epoch, int genBas
       return;
     }
     if (!gridSync(c, epoch)) return;
-    for (long long v = tid; v < n; v += T) {
-      if (isRoot(P.source, P.sources, P.nSources, static_cast<int>(v))) continue;
-      for (int k = 0; k < P.combK; ++k) {
-        int p, w;
-        if (combinedEdge(P, static_cast<int>(v), k, p, w)) {
-          const int pos = atomicAdd(P.combDeg + p, 1);
-          P.combCol[pos] = static_cast<int>(v);
-          P.combW[pos] = w;
+    for (long long v0 = tid; v0 < n; v0 += 4 * T) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const long long v = v0 + q * T;
+        if (v >= n || isRoot(P.source, P.sources, P.nSources, static_cast<int>(v))) continue;
+        for (int k = 0; k < P.combK; ++k) {
+          int p, w;
+          if (combinedEdge(P, static_cast<int>(v), k, p, w)) {
+            const int pos = atomicAdd(P.combDeg + p, 1);
+            P.combCol[pos] = static_cast<int>(v);
+            P.combW[pos] = w;
+          }
         }
       }
     }
@@ -2339,9 +2351,11 @@ __device__ void scratchOrCombined(const EngineParams &P, Sync &epoch, int genBas
   }
 
   // ---- SSSP from scratch: only the source (the roots) is finite ------------
+  bool heavyRow = false;  // one store at the end, so the loads run ahead
   for (long long v = tid; v < n; v += T) {
-    if (ldGraph<Mode>(outRow + v + 1) - ldGraph<Mode>(outRow + v) > heavyDegOf(P)) c->heavy = 1;
+    heavyRow |= ldGraph<Mode>(outRow + v + 1) - ldGraph<Mode>(outRow + v) > heavyDegOf(P);
   }
+  if (heavyRow) c->heavy = 1;
   for (int k = 0; k < K; ++k) {
     const Pk pk = pkOf(P.obj[k]);
     const long long ko = static_cast<long long>(k) * P.stride;
