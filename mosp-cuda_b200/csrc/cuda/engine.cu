@@ -2236,6 +2236,29 @@ __global__ void __launch_bounds__(kThreads, 1) sospEngine(const __grid_constant_
 }
 
 /// Steps 2-3 (combined mode) and the SSSP from scratch (both modes).
+/// The combined edges into v of every tree at once, for combK <= 8: the K
+/// parents are loaded once (combinedEdge reloads them per tree); has[k],
+/// p[k] and w[k] are what combinedEdge(P, v, k, ...) gives.
+__device__ __forceinline__ void combinedEdges8(const EngineParams &P, int v, int (&p)[8],
+                                               int (&w)[8], bool (&has)[8]) {
+  const long long n = P.n;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) p[k] = k < P.combK ? __ldg(P.combParents + k * n + v) : -1;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    bool first = p[k] >= 0;
+#pragma unroll
+    for (int j = 0; j < k; ++j) first = first && p[j] != p[k];
+    int weight = P.combBase - P.prefTerms[k];
+#pragma unroll
+    for (int j = k + 1; j < 8; ++j) {
+      if (p[j] == p[k]) weight -= P.prefTerms[j];  // trees past combK hold -1
+    }
+    has[k] = first;
+    w[k] = weight;
+  }
+}
+
 template <int Mode>
 __device__ void scratchOrCombined(const EngineParams &P, Sync &epoch, int genBase,
                                   const int **sOutWk) {
@@ -2257,7 +2280,25 @@ __device__ void scratchOrCombined(const EngineParams &P, Sync &epoch, int genBas
     // fill passes, so their parent loads and atomics are in flight together
     unsigned long long edges = 0, wsum = 0;
     bool badParent = false;
-    for (long long v0 = tid; v0 < n; v0 += 4 * T) {
+    const bool regs = P.combK <= 8;  // the same for every thread
+    for (long long v = tid; regs && v < n; v += T) {
+      if (isRoot(P.source, P.sources, P.nSources, static_cast<int>(v))) continue;
+      int p[8], w[8];
+      bool has[8];
+      combinedEdges8(P, static_cast<int>(v), p, w, has);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        if (!has[k]) continue;
+        if (p[k] >= n) {
+          badParent = true;
+          continue;
+        }
+        atomicAdd(P.combDeg + p[k], 1);
+        ++edges;
+        wsum += static_cast<unsigned long long>(w[k]);
+      }
+    }
+    for (long long v0 = tid; !regs && v0 < n; v0 += 4 * T) {
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         const long long v = v0 + q * T;
@@ -2296,7 +2337,20 @@ __device__ void scratchOrCombined(const EngineParams &P, Sync &epoch, int genBas
       return;
     }
     if (!gridSync(c, epoch)) return;
-    for (long long v0 = tid; v0 < n; v0 += 4 * T) {
+    for (long long v = tid; regs && v < n; v += T) {
+      if (isRoot(P.source, P.sources, P.nSources, static_cast<int>(v))) continue;
+      int p[8], w[8];
+      bool has[8];
+      combinedEdges8(P, static_cast<int>(v), p, w, has);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        if (!has[k]) continue;
+        const int pos = atomicAdd(P.combDeg + p[k], 1);
+        P.combCol[pos] = static_cast<int>(v);
+        P.combW[pos] = w[k];
+      }
+    }
+    for (long long v0 = tid; !regs && v0 < n; v0 += 4 * T) {
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         const long long v = v0 + q * T;
