@@ -2534,34 +2534,43 @@ __global__ void __launch_bounds__(kThreads, 1) pathCosts(const __grid_constant__
 
   for (long long v = tid; v < n; v += T) C.edgeOf[v] = INT_MAX;
   if (!gridSync(c, epoch)) return;
-  // first occurrence of the tree edge (parent[v], v): lowest e in row p
-  for (long long base = gwarp * 32; base < n; base += nwarps * 32) {
-    const long long u = base + lane;
-    int beg = 0, end = 0;
-    if (u < n) {
-      beg = __ldg(C.outRow + u);
-      end = __ldg(C.outRow + u + 1);
-    }
-    const int deg = end - beg;
-    unsigned big = __ballot_sync(kFull, deg > kLaneRowMax);
-    if (deg <= kLaneRowMax) {
-      for (int e = beg; e < end; ++e) {
-        const int v = __ldg(C.outCol + e);
-        if (!isRoot(C.source, C.sources, C.nSources, v) && __ldg(C.parent + v) == u) {
-          atomicMin(C.edgeOf + v, e);
-        }
+  // first occurrence of the tree edge (parent[v], v): lowest e in row p.
+  // Edge-balanced: warp w takes the w-th equal slice of the edge array and
+  // finds the row of each of its 32 edges from the ends of the next 32 rows
+  // (one coalesced load, a 5-step shuffle search), so hub rows are shared
+  // by many warps instead of walked by one.
+  {
+    const long long m = __ldg(C.outRow + n);
+    const long long wb = m * gwarp / nwarps, we = m * (gwarp + 1) / nwarps;
+    if (wb < we) {  // the same for the whole warp
+      int lo = 0, hi = n;  // the row of the slice's first edge: last r with row[r] <= wb
+      while (hi - lo > 1) {
+        const int mid = lo + ((hi - lo) >> 1);
+        if (__ldg(C.outRow + mid) <= wb) lo = mid; else hi = mid;
       }
-    }
-    while (big != 0) {
-      const int src = __ffs(big) - 1;
-      big &= big - 1;
-      const int ub = static_cast<int>(__shfl_sync(kFull, u, src));
-      const int bb = __shfl_sync(kFull, beg, src);
-      const int eb = __shfl_sync(kFull, end, src);
-      for (int e = bb + static_cast<int>(lane); e < eb; e += 32) {
-        const int v = __ldg(C.outCol + e);
-        if (!isRoot(C.source, C.sources, C.nSources, v) && __ldg(C.parent + v) == ub) {
-          atomicMin(C.edgeOf + v, e);
+      int r0 = lo;
+      for (long long e0 = wb; e0 < we; e0 += 32) {
+        const bool valid = e0 + lane < we;
+        const int e = static_cast<int>(e0 + lane);
+        const int x = valid ? __ldg(C.outCol + e) : 0;
+        int row = valid ? -1 : 0;
+        for (int base = r0; base < n; base += 32) {
+          const int rr = base + static_cast<int>(lane);
+          const int end = rr < n ? __ldg(C.outRow + rr + 1) : INT_MAX;
+          int pos = 0;  // rows of the window that end at or before e
+#pragma unroll
+          for (int step = 16; step >= 1; step >>= 1) {
+            if (__shfl_sync(kFull, end, pos + step - 1) <= e) pos += step;
+          }
+          // every lane takes part in the shuffle, found or not
+          const int lastEnd = __shfl_sync(kFull, end, 31);
+          if (row < 0 && e < lastEnd) row = base + pos;
+          if (__all_sync(kFull, row >= 0)) break;
+        }
+        r0 = __shfl_sync(kFull, row, 31);  // the largest row; past the slice the loop ends
+        if (valid && row >= 0 && row < n && static_cast<unsigned>(x) < static_cast<unsigned>(n) &&
+            !isRoot(C.source, C.sources, C.nSources, x) && __ldg(C.parent + x) == row) {
+          atomicMin(C.edgeOf + x, e);
         }
       }
     }
