@@ -95,7 +95,7 @@ TreeCheck checkSospTree(const CsrGraph &reverse, int objective, int source,
                         const std::vector<long long> &referenceDistances,
                         const std::vector<int> *referenceParents) {
   const int n = reverse.numberOfNodes;
-  auto judge = [&](int lo, int hi) {
+  auto checkRange = [&](int lo, int hi) {
     RangeVerdict r;
     for (int v = lo; v < hi; ++v) {
       const long long dv = distances[v], rv = referenceDistances[v];
@@ -122,11 +122,11 @@ TreeCheck checkSospTree(const CsrGraph &reverse, int objective, int source,
   std::vector<std::thread> pool;
   for (int t = 1; t < workers; ++t) {
     pool.emplace_back([&, t] {
-      part[t] = judge(static_cast<int>(static_cast<long long>(n) * t / workers),
+      part[t] = checkRange(static_cast<int>(static_cast<long long>(n) * t / workers),
                       static_cast<int>(static_cast<long long>(n) * (t + 1) / workers));
     });
   }
-  part[0] = judge(0, static_cast<int>(static_cast<long long>(n) / workers));
+  part[0] = checkRange(0, static_cast<int>(static_cast<long long>(n) / workers));
   for (std::thread &th : pool) th.join();
   TreeCheck check;
   for (const RangeVerdict &r : part) {
